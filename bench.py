@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark: one synchronous label-propagation iteration over a CGR graph.
+
+Metric: decoded arcs x iterations per second (every stored arc is decoded and
+its label counted once per iteration), with the roofline of the dominant
+kernel against the measured HBM copy bandwidth.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rmat-s24]
+    python bench.py --impl reference ...   # the CPU path (oracle port), same metric
+
+Multi-GPU: one process per GPU (torchrun); every rank runs an independent
+replica of the workload (the path has no exchange step on one graph);
+value = the arcs all ranks processed / the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "decoded arcs×iters/sec"
+UNIT = "arcs*iters/s"
+L2_BYTES = 126 * 1024 * 1024
+
+WORKLOADS = {
+    # R-MAT scale 24, edge factor 16 (a,b,c,d = .57,.19,.19,.05), symmetrised,
+    # de-duplicated, loops dropped, BFS relabelled; CGR threshold 32; sketch at >= 1024
+    "rmat-s24": dict(kind="rmat", scale=24, edge_factor=16.0, seed=1, small_thresh=32, cms=1024, iters=20),
+    # road-like grid 1404x1404, p=0.7, 2% extras within distance 3, threshold 0
+    "road-1404": dict(kind="road", width=1404, height=1404, seed=1, small_thresh=0, cms=0, iters=30),
+    # road-like grid 362x362 (the reference's CPU-runnable case)
+    "road-362": dict(kind="road", width=362, height=362, seed=1, small_thresh=0, cms=0, iters=20),
+    # smaller R-MAT for quick checks
+    "rmat-s20": dict(kind="rmat", scale=20, edge_factor=16.0, seed=1, small_thresh=32, cms=1024, iters=20),
+}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Maximum of a per-rank scalar over all ranks (the slowest rank's time)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int, device=None):
+    if world > 1:
+        import torch.distributed as dist
+
+        if device is not None and str(device).startswith("cuda"):
+            dist.barrier(device_ids=[int(str(device).split(":")[1])])
+        else:
+            dist.barrier()
+
+
+def build_graph(w: dict):
+    import lpa_b200 as L
+
+    if w["kind"] == "rmat":
+        g = L.HostGraph.rmat(w["scale"], w["edge_factor"], seed=w["seed"])
+    else:
+        g = L.HostGraph.road(w["width"], w["height"], seed=w["seed"])
+    g.compress(w["small_thresh"], 128)
+    return g
+
+
+def shared_graph_arrays(name: str, w: dict, rank: int, world: int, device=None) -> dict:
+    """Rank 0 builds the workload; under torchrun the other ranks load rank 0's
+    arrays from /dev/shm instead of regenerating them."""
+    import lpa_b200 as L
+
+    if world <= 1:
+        return build_graph(w).arrays()
+    d = Path("/dev/shm") / f"lpa_bench_{name}"
+    if rank == 0:
+        arr = build_graph(w).arrays()
+        d.mkdir(exist_ok=True)
+        for k, v in arr.items():
+            if isinstance(v, np.ndarray):
+                np.save(d / f"{k}.npy", v)
+        (d / "meta.json").write_text(json.dumps({"n": arr["n"], "n_c": arr["n_c"]}))
+    barrier(world, device)
+    if rank != 0:
+        meta = json.loads((d / "meta.json").read_text())
+        arr = dict(meta)
+        for k in ("words", "offsets", "vertices", "small_graph", "small_offset"):
+            arr[k] = np.load(d / f"{k}.npy")
+    barrier(world, device)
+    return arr
+
+
+class ClockSampler:
+    """nvidia-smi samples (SM clock, reasons) while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-i", str(device_index), "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, r[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_gbs():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def traffic_summary(workload: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get(workload)
+        except Exception:
+            return None
+    return None
+
+
+def segment_bytes(arr: dict, deg: np.ndarray, seg_b, seg_e, seg_v) -> dict:
+    """Algorithmic bytes per variant: stream bits of its compressed positions,
+    8 B offset + 4 B id + 4 B degree per compressed position, the small CSR of
+    its CSR positions (4 B offset + 4 B per arc), 8 B label read+write per vertex."""
+    n_c = arr["n_c"]
+    off = arr["offsets"].astype(np.int64)
+    out = {v: 0 for v in range(4)}
+    arcs = {v: 0 for v in range(4)}
+    cs = np.concatenate([[0], np.cumsum(deg.astype(np.int64))])
+    for b, e, v in zip(seg_b.tolist(), seg_e.tolist(), seg_v.tolist()):
+        k = e - b
+        if b < n_c:
+            bits = int(off[e] - off[b])
+            out[v] += (bits + 7) // 8 + 16 * k + 8 * k
+        else:
+            out[v] += 8 * k + 4 * int(cs[e] - cs[b]) + 8 * k
+        arcs[v] += int(cs[e] - cs[b])
+    return {"bytes": out, "arcs": arcs}
+
+
+def cpu_baseline(arr: dict, w: dict, budget_s: float = 12.0) -> dict:
+    """The oracle's OpenMP CPU path (decode + synchronous LP, same rule) on a
+    bounded sample of the same workload: a prefix of the positions."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    n = arr["n"]
+    lab = np.arange(n, dtype=np.uint32)
+    p_end = min(n, 1 << 14)
+    while True:
+        t0 = time.perf_counter()
+        oracle.lp_iterate_cgr(arr, lab, w["cms"], 1, threads, 0, p_end)
+        dt = time.perf_counter() - t0
+        if dt > budget_s / 8 or p_end >= n:
+            break
+        p_end = min(n, p_end * 4)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        oracle.lp_iterate_cgr(arr, lab, w["cms"], 1, threads, 0, p_end)
+        times.append(time.perf_counter() - t0)
+    row_arcs = oracle.range_arcs(arr, 0, p_end)
+    t = statistics.median(times)
+    return {"value": row_arcs / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"positions [0,{p_end}) of {n} ({row_arcs} arcs), median of 3 iterations after 1 warm-up"}
+
+
+def run_reference(args, w, rank, world):
+    if rank != 0:
+        return
+    arr = build_graph(w).arrays()
+    cb = cpu_baseline(arr, w, budget_s=20.0)
+    steps = args.steps
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": 0, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.workload, "n": arr["n"], "small_thresh": w["small_thresh"],
+                       "cms_threshold": w["cms"], "parallelism": "cpu-openmp"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat-s24", choices=sorted(WORKLOADS))
+    ap.add_argument("--dispatch", default="fixed", choices=["fixed", "learned"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    w = WORKLOADS[args.workload]
+    rank, world, local = dist_env()
+
+    if args.impl == "reference":
+        run_reference(args, w, rank, world)
+        return
+
+    import torch
+
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=torch.device(device))
+
+    import lpa_b200 as L
+
+    arr = shared_graph_arrays(args.workload, w, rank, world, device)
+    stream = torch.cuda.Stream(device=device)
+    p = L.Propagator(L.desc_from_arrays(arr), device=local, cms_threshold=w["cms"], cms_seed=1,
+                     record_timings=1, stream=stream.cuda_stream,
+                     dispatch=L.Dispatch.FIXED)
+    info = p.get_info()
+    arcs = int(info.num_arcs)
+    b_alg = int(info.bytes_algorithmic)
+    inputs_bytes = b_alg
+    flush = inputs_bytes < 2 * L2_BYTES
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=device) if flush else None
+
+    # warm-up
+    p.init_labels()
+    for _ in range(args.warmup):
+        p.iterate()
+
+    st0 = p.stats()
+    barrier(world, device)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    wall0 = time.perf_counter()
+    dev_ms = 0.0
+    var_ms = np.zeros(4)
+    for _ in range(args.steps):
+        if flush:
+            with torch.cuda.stream(stream):
+                flush_buf.fill_(1)
+        p.iterate()
+        s = p.stats()
+        dev_ms += s.last_iter_ms
+        var_ms += np.array(list(s.variant_ms))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    barrier(world, device)
+    st1 = p.stats()
+    total_ms = max_over_ranks(dev_ms, world, device)
+    value = arcs * args.steps * world / (total_ms / 1e3)
+    ms_per_step = total_ms / args.steps
+
+    # dominant kernel roofline
+    deg = p.degrees()
+    sb, se, sbk, sv = p.segments()
+    per = segment_bytes(arr, deg, sb, se, sv)
+    var_avg_ms = var_ms / args.steps
+    dom = int(np.argmax(var_avg_ms))
+    peak, peak_kind = measured_peak_gbs()
+    dom_bytes = per["bytes"][dom]
+    achieved = dom_bytes / (var_avg_ms[dom] / 1e3) / 1e9 if var_avg_ms[dom] > 0 else 0.0
+    iter_achieved = b_alg / (ms_per_step / 1e3) / 1e9
+    names = {0: "warp", 1: "packed", 2: "block", 3: "two_pass"}
+
+    # end to end through the C ABI with host buffers (pinned)
+    host_in = torch.empty(arr["n"], dtype=torch.int32, pin_memory=True)
+    host_out = torch.empty(arr["n"], dtype=torch.int32, pin_memory=True)
+    host_in.copy_(torch.from_numpy(p.labels().view(np.int32)))
+    import ctypes as C
+
+    lib = L.lib()
+    in_ptr = C.cast(C.c_void_p(host_in.data_ptr()), C.POINTER(C.c_uint32))
+    out_ptr = C.cast(C.c_void_p(host_out.data_ptr()), C.POINTER(C.c_uint32))
+    chg = C.c_uint64()
+    barrier(world, device)
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        assert lib.lpa_set_labels(p._h, in_ptr, arr["n"]) == 0
+        assert lib.lpa_iterate(p._h, C.byref(chg)) == 0
+        assert lib.lpa_get_labels(p._h, out_ptr, arr["n"]) == 0
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - e0, world, device)
+    e2e_value = arcs * args.e2e_steps * world / e2e_s
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(arr, w)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": args.workload, "n": arr["n"], "arcs": arcs, "compressed": arr["n_c"],
+                       "stream_bytes": (int(info.stream_bits) + 7) // 8, "small_thresh": w["small_thresh"],
+                       "cms_threshold": w["cms"], "dispatch": args.dispatch,
+                       "l2": "L2 flushed between iterations" if flush else "inputs larger than L2",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "bytes_per_launch": dom_bytes, "ms_per_launch": float(var_avg_ms[dom]),
+                         "traffic": traffic_summary(args.workload),
+                         "iteration": {"bytes": b_alg, "achieved": iter_achieved, "frac": iter_achieved / peak},
+                         "variant_ms": {names[v]: float(var_avg_ms[v]) for v in range(4)}},
+            "cpu_baseline": cb,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * arr["n"],
+                    "d2h_bytes_per_step": 4 * arr["n"] + 8},
+            "gpu_launches": int(st1.launches - st0.launches),
+            "clocks": clk,
+            "wall_s_timed": wall,
+        }
+        print(json.dumps(line), flush=True)
+    p.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

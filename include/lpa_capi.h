@@ -1,0 +1,202 @@
+/*
+ * lpa_capi.h -- C ABI of the B200 label-propagation library (liblpa_b200.so).
+ *
+ * One synchronous label-propagation iteration over a CGR-compressed graph,
+ * run by hand-written sm_100a kernels.  Plain pointers and sizes only; every
+ * call returns an lpa_status and no exception crosses the boundary.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   - the propagator classes NovaPlusPropagator / NovaPropagator /
+ *     CGLPPropagator: run(), iterate(), get_labels(), preprocess(),
+ *     transfer_data() (baselines/novaplus/novaplus_propogator.cuh:100-199,
+ *     :340-373; baselines/cglp/cglp_propagator.cuh:205-335;
+ *     include/label_propagator.h:26-33);
+ *   - the kernels they launch (baselines/novaplus/kernel.cuh:14-191,
+ *     include/decoder.cuh:50-1025) -- reached only through these entry points;
+ *   - the GPU decompress test harness (include/decompressor.cuh:116-144,
+ *     test/decompress_test.cu:42-79) -> lpa_decode_csr;
+ *   - the CPU format layer (src/compressor.cpp, src/file.cpp) -> lpa_hg_*.
+ *
+ * Ownership: host buffers passed in are copied; the caller keeps them.
+ * Device memory belongs to the handle.  Threading: a handle is not
+ * thread-safe; separate handles may be used from separate threads.
+ */
+#ifndef LPA_CAPI_H
+#define LPA_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum lpa_status {
+  LPA_OK = 0,
+  LPA_ERR_CUDA = 1,        /* a CUDA runtime call failed */
+  LPA_ERR_OOM = 2,         /* a device allocation failed */
+  LPA_ERR_BAD_STREAM = 3,  /* the decoder left a vertex's bit range, or an id >= n */
+  LPA_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+  LPA_ERR_INVALID_ARG = 5, /* bad pointer, size or option */
+  LPA_ERR_IO = 6,          /* a file is missing or malformed */
+  LPA_ERR_NO_DEVICE = 7,   /* no usable CUDA device */
+  LPA_ERR_CAPACITY = 8     /* a work item exceeded a planned capacity (internal) */
+} lpa_status;
+
+/* Kernel variants.  All of them produce identical labels. */
+typedef enum lpa_variant {
+  LPA_VARIANT_WARP = 0,     /* V1: warp per vertex (degree <= 256)              */
+  LPA_VARIANT_PACKED = 1,   /* V2: several vertices per warp (degree <= 32)     */
+  LPA_VARIANT_BLOCK = 2,    /* V3: block per vertex                             */
+  LPA_VARIANT_TWO_PASS = 3  /* V4: decode to a CSR scratch, then propagate      */
+} lpa_variant;
+
+typedef enum lpa_dispatch {
+  LPA_DISPATCH_FIXED = 0,   /* degree buckets: <16 packed, <128 warp, >=128 block */
+  LPA_DISPATCH_LEARNED = 1, /* MLP cost model over segment features, judged by FIXED */
+  LPA_DISPATCH_FORCE = 2    /* force_variant wherever it is capable, FIXED elsewhere */
+} lpa_dispatch;
+
+/* The compressed mixed graph: the content of the reference's .graph, .offset,
+ * .vertices.bin, .graph.small.bin and .offset.small.bin files (File::
+ * load_graph, src/file.cpp:24-74), with 64-bit bit offsets. */
+typedef struct lpa_graph_desc {
+  uint64_t num_vertices;        /* n = number of positions in vertices[] */
+  uint64_t num_compressed;      /* n_c: positions [0, n_c) are in the bitstream */
+  const uint32_t *words;        /* bitstream as big-endian 32-bit words (File::graph) */
+  uint64_t num_words;
+  const uint64_t *offsets;      /* n_c + 1 bit offsets, offsets[0] = 0 */
+  const uint32_t *vertices;     /* position -> vertex id, n entries */
+  const uint32_t *small_graph;  /* neighbours of positions >= n_c (CSR) */
+  uint64_t num_small_arcs;
+  const uint32_t *small_offset; /* n - n_c + 1 entries; NULL when n == n_c */
+} lpa_graph_desc;
+
+typedef struct lpa_opts {
+  int device;              /* CUDA device ordinal */
+  uint32_t cms_threshold;  /* degree >= this uses the count-min sketch; 0: never */
+  uint64_t cms_seed;       /* seeds the sketch's row hashes */
+  int dispatch;            /* lpa_dispatch */
+  int force_variant;       /* lpa_variant, with LPA_DISPATCH_FORCE */
+  void *stream;            /* cudaStream_t to run on; NULL: the handle makes one */
+  int record_timings;      /* per-segment device cycles and per-launch events */
+  int verbose;             /* per-iteration log lines on stdout */
+} lpa_opts;
+
+typedef struct lpa_info {
+  uint64_t num_vertices, num_compressed, num_arcs, num_small_arcs;
+  uint64_t stream_bits;
+  uint64_t num_segments;
+  uint64_t max_degree;
+  uint64_t bytes_algorithmic; /* one iteration's compulsory bytes (see lpa_info docs) */
+  uint64_t device_bytes;      /* device memory held by the handle */
+} lpa_info;
+
+typedef struct lpa_stats {
+  uint64_t iterations;              /* iterations run since lpa_init_labels */
+  uint64_t last_changed;            /* changed count of the last iteration */
+  double last_iter_ms;              /* device time of the last iteration */
+  double variant_ms[4];             /* device time per variant, last iteration */
+  uint64_t variant_segments[4];     /* segments assigned per variant */
+  uint64_t variant_arcs[4];         /* arcs assigned per variant */
+  double mlp_loss;                  /* last training loss of the cost model */
+  uint64_t mlp_updates;             /* SGD steps taken */
+  uint64_t dispatch_reverts;        /* times the learned plan was judged slower */
+  int learned_active;               /* 1 when the learned plan is in use */
+  uint64_t launches;                /* kernel launches enqueued by this handle */
+} lpa_stats;
+
+/* ---------------------------------------------------------------- basics -- */
+const char *lpa_status_str(lpa_status s);
+const char *lpa_version(void);
+void lpa_opts_default(lpa_opts *o);
+
+/* --------------------------------------------------- propagator handle ---- */
+/* Copies the graph to the device, derives every compressed vertex's degree by
+ * decoding it once, and builds the dispatch plan.  Replaces
+ * NovaPlusPropagator::preprocess / transfer_data
+ * (baselines/novaplus/novaplus_propogator.cuh:201-204,340-373). */
+lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, struct lpa_handle **out);
+lpa_status lpa_destroy(struct lpa_handle *h);
+lpa_status lpa_get_info(struct lpa_handle *h, lpa_info *info);
+const char *lpa_last_error(struct lpa_handle *h);
+
+/* L[v] = v (initialize_labels, baselines/novaplus/kernel.cuh:57-64). */
+lpa_status lpa_init_labels(struct lpa_handle *h);
+/* Sets the current labels from host memory (n entries). */
+lpa_status lpa_set_labels(struct lpa_handle *h, const uint32_t *host, size_t n);
+/* One synchronous iteration; *changed_out (may be NULL) receives the number
+ * of vertices whose label changed.  Replaces NovaPlusPropagator::iterate
+ * (baselines/novaplus/novaplus_propogator.cuh:131-199). */
+lpa_status lpa_iterate(struct lpa_handle *h, uint64_t *changed_out);
+/* Runs up to max_iter iterations; with early_exit it stops after an iteration
+ * that changed nothing (device-side test inside a CUDA graph).  Replaces
+ * NovaPlusPropagator::run (baselines/novaplus/novaplus_propogator.cuh:100-129). */
+lpa_status lpa_run(struct lpa_handle *h, int max_iter, int early_exit, int *iters_done);
+/* Per-iteration changed counts of the last lpa_run (count entries). */
+lpa_status lpa_get_changed_history(struct lpa_handle *h, uint64_t *out, size_t count);
+/* Copies the current labels to host memory (n entries).  Replaces
+ * LabelPropagator::get_labels (include/label_propagator.h:30-35). */
+lpa_status lpa_get_labels(struct lpa_handle *h, uint32_t *host_out, size_t n);
+lpa_status lpa_get_stats(struct lpa_handle *h, lpa_stats *st);
+
+/* Decodes the whole graph on the device into a CSR indexed by vertex id:
+ * row_out has n + 1 entries, clm_out num_arcs entries; each list holds the
+ * interval neighbours then the residual neighbours, each part ascending (sort
+ * a list to compare with the reference's .clm).  Parity hook replacing the
+ * decompress test harness (include/decompressor.cuh:116-144). */
+lpa_status lpa_decode_csr(struct lpa_handle *h, uint64_t *row_out, uint32_t *clm_out);
+
+/* Degree of every position as decoded on the device (n entries). */
+lpa_status lpa_get_degrees(struct lpa_handle *h, uint32_t *deg_out, size_t n);
+
+/* Dispatch control.  Assign a variant to one segment (-1: all segments whose
+ * degrees it supports), rebuilding the launch lists. */
+lpa_status lpa_set_dispatch(struct lpa_handle *h, int dispatch, int force_variant);
+/* Per-segment view of the plan: begin/end positions, bucket, variant. */
+lpa_status lpa_get_segments(struct lpa_handle *h, uint32_t *begin, uint32_t *end, uint8_t *bucket,
+                            uint8_t *variant, size_t count);
+
+/* ------------------------------------------ host format layer (lpa_hg_*) --- */
+/* A host graph owns a CSR (by vertex id) and/or its compressed form, produced
+ * by the fast bit-identical encoder that replaces CgrCompressor
+ * (src/compressor.cpp:70-515) and File (src/file.cpp:24-262). */
+typedef struct lpa_host_graph lpa_host_graph;
+
+lpa_status lpa_hg_generate_road(uint32_t width, uint32_t height, double keep_p, double extra_p,
+                                int max_dist, uint64_t seed, lpa_host_graph **out);
+lpa_status lpa_hg_generate_rmat(int scale, double edge_factor, double a, double b, double c,
+                                uint64_t seed, int bfs_relabel, uint64_t n_limit, lpa_host_graph **out);
+lpa_status lpa_hg_generate_copy(uint64_t n, uint32_t out_degree, double copy_p, int copy_offset,
+                                double zipf_s, uint64_t seed, lpa_host_graph **out);
+/* Takes a CSR (lists sorted, no duplicates). */
+lpa_status lpa_hg_from_csr(uint64_t n, const uint64_t *row, const uint32_t *clm, lpa_host_graph **out);
+/* Reference edge-list ingest (File::read_from_edge_list, src/file.cpp:115-195). */
+lpa_status lpa_hg_read_edge_list(const char *path, int one_way, lpa_host_graph **out);
+/* Reference edge list written back out (both arcs, or each edge once). */
+lpa_status lpa_hg_write_edge_list(lpa_host_graph *g, const char *path, int both_arcs);
+/* CgrCompressor(3, 4, 256, 256) + write_cgr(path, small_thresh, large_thresh). */
+lpa_status lpa_hg_compress(lpa_host_graph *g, int small_thresh, int large_thresh, int threads);
+/* Loads the reference's compressed files (64-bit offsets). */
+lpa_status lpa_hg_load_cgr(const char *base, int small_thresh, lpa_host_graph **out);
+lpa_status lpa_hg_write_cgr(lpa_host_graph *g, const char *base);
+/* Reference .row/.clm. */
+lpa_status lpa_hg_write_csr(lpa_host_graph *g, const char *base);
+lpa_status lpa_hg_csr(lpa_host_graph *g, uint64_t *n, const uint64_t **row, const uint32_t **clm);
+/* Fills desc with pointers into g (valid while g lives). */
+lpa_status lpa_hg_desc(lpa_host_graph *g, lpa_graph_desc *desc);
+lpa_status lpa_hg_free(lpa_host_graph *g);
+
+/* ------------------------------------------------- batched graphs ---------- */
+/* Many independent graphs propagated by one persistent kernel fed from a
+ * device work queue, each with its own convergence test. */
+lpa_status lpa_batch_create(const lpa_graph_desc *graphs, size_t num_graphs, const lpa_opts *o,
+                            struct lpa_batch **out);
+lpa_status lpa_batch_run(struct lpa_batch *b, int max_iter, int early_exit, uint32_t *iters_per_graph);
+lpa_status lpa_batch_get_labels(struct lpa_batch *b, size_t graph, uint32_t *host_out, size_t n);
+lpa_status lpa_batch_destroy(struct lpa_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LPA_CAPI_H */

@@ -1,0 +1,244 @@
+// Device-side CGR decode primitives and shared helpers (sm_100a).
+//
+// The bit reader restates the reference's CgrReader (include/graph_utils.cuh:
+// 19-98) with 64-bit bit positions and a 64-bit window, so one window serves
+// any gamma code (<= 63 bits) or zeta_3 code (<= 44 bits) of a 32-bit value.
+// Every read position is checked against the vertex's bit range by the
+// callers; a violation sets the device error word (never traps).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lpa_dev {
+
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+constexpr uint32_t kSegBits = 256;  // INTERVAL_SEGMENT_LEN, graph_utils.cuh:17
+constexpr uint32_t kMinItv = 4;     // minimum interval length, graph_utils.cuh:172
+constexpr int kCmsDepth = 4;
+constexpr uint32_t kCmsWidth = 1024;
+
+// device error word values (first error wins)
+enum : uint32_t {
+  kErrNone = 0,
+  kErrBadStream = 1,  // a decode left the vertex's bit range or produced an id >= n
+  kErrCapacity = 2,   // more items than a staging buffer was planned for
+  kErrTimeout = 3,    // a bounded wait gave up
+};
+
+__device__ __forceinline__ void set_error(uint32_t *err, uint32_t code) {
+  if (err) atomicCAS(err, kErrNone, code);
+}
+
+// Bitstream and mixed-graph arrays as the kernels see them.
+struct DevGraph {
+  const uint32_t *words;     // stream words (big-endian packing), >= 4 zero words of tail
+  const uint64_t *offsets;   // n_c + 1 bit offsets by position
+  const uint32_t *vertices;  // position -> vertex id (n)
+  const uint32_t *deg;       // position -> degree (n)
+  const uint32_t *small_off; // small CSR offsets by (position - n_c), n - n_c + 1
+  const uint32_t *small_nbr; // small CSR neighbours
+  uint64_t n;                // vertices
+  uint64_t n_c;              // compressed vertices
+};
+
+// 64 stream bits starting at bit `pos`, MSB first.
+template <class W>
+__device__ __forceinline__ uint64_t win64(W w, uint64_t pos) {
+  const uint64_t i = pos >> 5;
+  const uint32_t s = uint32_t(pos) & 31u;
+  const uint32_t a = w(i), b = w(i + 1), c = w(i + 2);
+  const uint32_t hi = __funnelshift_l(b, a, s);
+  const uint32_t lo = __funnelshift_l(c, b, s);
+  return (uint64_t(hi) << 32) | lo;
+}
+
+// Global-memory word source (read-only path).
+struct GWords {
+  const uint32_t *__restrict__ p;
+  __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return __ldg(p + i); }
+};
+
+// Shared-memory word source: words [base_word, base_word + len) staged at s.
+struct SWords {
+  const uint32_t *s;
+  uint64_t base_word;
+  __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return s[i - base_word]; }
+};
+
+// gamma (graph_utils.cuh:63-67): z zeros, then the z+1 bits of x+1.
+template <class W>
+__device__ __forceinline__ uint32_t dec_gamma(W w, uint64_t &pos, bool &bad) {
+  const uint64_t x = win64(w, pos);
+  const uint32_t z = __clzll(x);
+  if (z > 31) {
+    bad = true;
+    return 0;
+  }
+  pos += 2 * z + 1;
+  return uint32_t(x >> (63 - 2 * z)) - 1u;
+}
+
+// zeta_3 (graph_utils.cuh:69-76): h zeros, a one, then 3(h+1) bits of x+1.
+template <class W>
+__device__ __forceinline__ uint32_t dec_zeta3(W w, uint64_t &pos, bool &bad) {
+  const uint64_t x = win64(w, pos);
+  const uint32_t h = __clzll(x);
+  if (h > 10) {
+    bad = true;
+    return 0;
+  }
+  pos += 4 * (h + 1);
+  return uint32_t((x << (h + 1)) >> (64 - 3 * (h + 1))) - 1u;
+}
+
+// decode_segment_cnt (graph_utils.cuh:88-97).
+template <class W>
+__device__ __forceinline__ uint32_t dec_segcnt(W w, uint64_t &pos, bool &bad) {
+  const uint64_t x = win64(w, pos);
+  const uint32_t z = __clzll(x);
+  if (z == 0) {  // gamma(0): one segment, unless the next bit marks it empty
+    if ((x >> 62) & 1ull) {
+      pos += 2;
+      return 0;
+    }
+    pos += 1;
+    return 1;
+  }
+  if (z > 31) {
+    bad = true;
+    return 0;
+  }
+  pos += 2 * z + 1;
+  return uint32_t(x >> (63 - 2 * z));  // gamma value + 1
+}
+
+// decode_first_num (graph_utils.cuh:34-37).
+__device__ __forceinline__ uint32_t zigzag_first(uint32_t node, uint32_t x) {
+  return (x & 1u) ? node - (x >> 1) - 1u : node + (x >> 1);
+}
+
+// Walks one vertex's neighbour list, calling emit(id) for every neighbour
+// (intervals first, then residuals).  Returns the count, or -1 on a stream
+// that leaves [pos, end), does not end at `end`, or names an id >= n.
+template <class W, class Emit>
+__device__ __forceinline__ int64_t walk_vertex(W w, uint64_t pos, uint64_t end, uint32_t node, uint64_t n,
+                                               Emit emit) {
+  bool bad = false;
+  int64_t cnt_all = 0;
+  // interval section (IntervalSegmentHelper, graph_utils.cuh:139-180)
+  uint32_t nseg = dec_segcnt(w, pos, bad);
+  const uint64_t ibase = pos;
+  uint64_t last = pos;
+  if (pos > end || nseg > (end - pos) / kSegBits + 1) return -1;
+  for (uint32_t j = 0; j < nseg && !bad; j++) {
+    uint64_t q = ibase + uint64_t(kSegBits) * j;
+    if (q >= end) return -1;
+    uint32_t cnt = dec_gamma(w, q, bad);
+    uint32_t left = 0;
+    for (uint32_t c = 0; c < cnt && !bad; c++) {
+      uint32_t l = dec_gamma(w, q, bad);
+      left = (c == 0) ? zigzag_first(node, l) : left + l + 1u;
+      uint32_t len = dec_gamma(w, q, bad) + kMinItv;
+      if (q > end || uint64_t(left) + len > n) return -1;
+      for (uint32_t k = 0; k < len; k++) emit(left + k);
+      cnt_all += len;
+      left += len;
+    }
+    last = q;
+  }
+  pos = last;
+  // residual section (ResidualSegmentHelper, graph_utils.cuh:100-137)
+  nseg = dec_segcnt(w, pos, bad);
+  const uint64_t rbase = pos;
+  last = pos;
+  if (pos > end || nseg > (end - pos) / kSegBits + 1) return -1;
+  for (uint32_t j = 0; j < nseg && !bad; j++) {
+    uint64_t q = rbase + uint64_t(kSegBits) * j;
+    if (q >= end) return -1;
+    uint32_t cnt = dec_gamma(w, q, bad);
+    uint32_t v = 0;
+    for (uint32_t c = 0; c < cnt && !bad; c++) {
+      uint32_t x = dec_zeta3(w, q, bad);
+      v = (c == 0) ? zigzag_first(node, x) : v + x + 1u;
+      if (q > end || uint64_t(v) >= n) return -1;
+      emit(v);
+      cnt_all++;
+    }
+    last = q;
+  }
+  if (bad || last != end) return -1;
+  return cnt_all;
+}
+
+// ---------------------------------------------------------------- hashing --
+// Count-min-sketch row hashes, include/cms.cuh:96-132 (cm_hash1..cm_hash4).
+__device__ __forceinline__ uint32_t cm_hash(int r, uint32_t k) {
+  switch (r) {
+    case 0:
+      k ^= k >> 16; k *= 0x12ebcb3bu; k ^= k >> 13; k *= 0xc123ae53u; k ^= k >> 16;
+      return k;
+    case 1:
+      k ^= k >> 16; k *= 0x21eb21bbu; k ^= k >> 13; k *= 0x2cb2ea35u; k ^= k >> 16;
+      return k;
+    case 2:
+      k ^= k >> 16; k *= 0x8febce61u; k ^= k >> 13; k *= 0xa2b2be25u; k ^= k >> 16;
+      return k;
+    default:
+      k ^= k >> 12; k *= 0x13ebdb3au; k ^= k >> 12; k *= 0xc123ae53u; k ^= k >> 14;
+      return k;
+  }
+}
+
+// Slot hash for the exact-count tables (a murmur3-style finaliser).
+__device__ __forceinline__ uint32_t slot_hash(uint32_t k) {
+  k ^= k >> 16;
+  k *= 0x7feb352du;
+  k ^= k >> 15;
+  k *= 0x846ca68bu;
+  k ^= k >> 16;
+  return k;
+}
+
+// (count, label) packed so that a larger value means a better label: more
+// occurrences first, then the smaller label.
+__device__ __forceinline__ uint64_t pack_best(uint32_t count, uint32_t label) {
+  return (uint64_t(count) << 32) | uint64_t(~label);
+}
+__device__ __forceinline__ uint32_t best_label(uint64_t packed) { return ~uint32_t(packed); }
+
+__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    uint64_t t = __shfl_xor_sync(kFull, v, o);
+    v = t > v ? t : v;
+  }
+  return v;
+}
+
+// Open-addressing exact counter in shared (or global) memory.  Keys are
+// stored as label + 1 so that 0 marks an empty slot.  cap is a power of two
+// larger than the number of distinct labels inserted.
+__device__ __forceinline__ void table_add(uint32_t *keys, uint32_t *cnts, uint32_t cap, uint32_t label,
+                                          uint32_t c) {
+  const uint32_t key = label + 1u;
+  uint32_t h = slot_hash(label) & (cap - 1);
+  for (uint32_t probe = 0; probe < cap; probe++) {
+    uint32_t k = keys[h];
+    if (k == key) {
+      atomicAdd(&cnts[h], c);
+      return;
+    }
+    if (k == 0) {
+      uint32_t old = atomicCAS(&keys[h], 0u, key);
+      if (old == 0u || old == key) {
+        atomicAdd(&cnts[h], c);
+        return;
+      }
+    }
+    h = (h + 1) & (cap - 1);
+  }
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+}  // namespace lpa_dev

@@ -1,0 +1,761 @@
+// C ABI implementation: device graph, dispatch plan and the iteration loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "lp_kernels.cuh"
+#include "lpa_capi.h"
+#include "runtime.h"
+
+using namespace lpa_dev;
+using namespace lpa_rt;
+
+namespace {
+
+constexpr int kMaxRunSlots = 1 << 16;
+
+// Segment cutting limits per bucket: positions and arcs.
+constexpr uint32_t kSegPositions[kNumBuckets] = {1024, 256, 64, 1};
+constexpr uint64_t kSegArcs = 16384;
+
+struct Fail {
+  lpa_status st;
+  std::string msg;
+};
+
+void check(lpa_handle *h, cudaError_t e, const char *where) {
+  if (e != cudaSuccess) {
+    lpa_status st = (e == cudaErrorMemoryAllocation) ? LPA_ERR_OOM : LPA_ERR_CUDA;
+    throw Fail{st, std::string(where) + ": " + cudaGetErrorString(e)};
+  }
+  (void)h;
+}
+
+template <class T>
+T *dalloc(lpa_handle *h, uint64_t count, const char *what) {
+  void *p = nullptr;
+  const uint64_t bytes = std::max<uint64_t>(count, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Fail{LPA_ERR_OOM, std::string("cudaMalloc ") + what + " (" + std::to_string(bytes) + " bytes)"};
+  }
+  h->allocations.push_back(p);
+  h->device_bytes += bytes;
+  return static_cast<T *>(p);
+}
+
+template <class T>
+void h2d(lpa_handle *h, T *dst, const T *src, uint64_t count, const char *what) {
+  if (count == 0) return;
+  check(h, cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, h->stream), what);
+}
+
+lpa_status guard(lpa_handle *h, const Fail &f) {
+  if (h) h->last_error = f.msg;
+  return f.st;
+}
+
+DevGraph dev_graph(const lpa_handle *h) {
+  DevGraph g;
+  g.words = h->d_words;
+  g.offsets = h->d_offsets;
+  g.vertices = h->d_vertices;
+  g.deg = h->d_deg;
+  g.small_off = h->d_small_off;
+  g.small_nbr = h->d_small_nbr;
+  g.n = h->n;
+  g.n_c = h->n_c;
+  return g;
+}
+
+void cms_seeds(uint64_t seed, uint32_t out[kCmsDepth]) {
+  // seed_r = low32(seed) ^ (0x9E3779B9 * (r + 1)), plus high32(seed) * 0x85EBCA6B
+  const uint32_t lo = uint32_t(seed), hi = uint32_t(seed >> 32);
+  for (int r = 0; r < kCmsDepth; r++) out[r] = (lo ^ (0x9E3779B9u * uint32_t(r + 1))) + hi * 0x85EBCA6Bu;
+}
+
+// Reads and clears the device error word.
+lpa_status take_device_error(lpa_handle *h) {
+  uint32_t err = 0;
+  check(h, cudaMemcpyAsync(&err, h->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream), "read error word");
+  check(h, cudaStreamSynchronize(h->stream), "synchronize");
+  if (err == kErrNone) return LPA_OK;
+  check(h, cudaMemsetAsync(h->d_err, 0, sizeof(uint32_t), h->stream), "clear error word");
+  switch (err) {
+    case kErrBadStream:
+      h->last_error = "bitstream decode left a vertex's bit range or produced an id >= n";
+      return LPA_ERR_BAD_STREAM;
+    case kErrCapacity:
+      h->last_error = "a vertex exceeded its variant's planned capacity";
+      return LPA_ERR_CAPACITY;
+    case kErrTimeout:
+      h->last_error = "a bounded device wait gave up";
+      return LPA_ERR_TIMEOUT;
+    default:
+      h->last_error = "unknown device error";
+      return LPA_ERR_CUDA;
+  }
+}
+
+}  // namespace
+
+namespace lpa_rt {
+
+bool variant_capable(int v, const SegInfo &s, uint32_t cms_thr) {
+  const bool any_cms = cms_thr != 0 && s.max_deg >= cms_thr;
+  switch (v) {
+    case LPA_VARIANT_PACKED:
+      return !any_cms && s.max_deg <= kV2MaxDeg;
+    case LPA_VARIANT_WARP:
+      return !any_cms && s.max_deg <= kV1MaxDeg;
+    case LPA_VARIANT_BLOCK:
+    case LPA_VARIANT_TWO_PASS:
+      return true;
+    default:
+      return false;
+  }
+}
+
+// The reference's degree buckets: <16 packed warp, <128 warp, >=128 block
+// (baselines/novaplus/novaplus_propogator.cuh:219-220, include/decoder.cuh:50-58).
+int fixed_variant(const SegInfo &s) {
+  switch (s.bucket) {
+    case kTiny:
+      return LPA_VARIANT_PACKED;
+    case kMid:
+      return LPA_VARIANT_WARP;
+    default:
+      return LPA_VARIANT_BLOCK;
+  }
+}
+
+}  // namespace lpa_rt
+
+// ------------------------------------------------------------------ plan ---
+static void build_segments(lpa_handle *h) {
+  h->segs.clear();
+  const uint32_t cms = h->opts.cms_threshold;
+  auto bucket_of = [&](uint32_t d) -> uint8_t {
+    if ((cms != 0 && d >= cms) || d > kV1MaxDeg) return kHeavy;
+    if (d < 16) return kTiny;
+    if (d < 128) return kMid;
+    return kLarge;
+  };
+  SegInfo cur{};
+  bool open = false;
+  auto close = [&]() {
+    if (open) h->segs.push_back(cur);
+    open = false;
+  };
+  for (uint64_t p = 0; p < h->n; p++) {
+    const uint32_t d = h->h_deg[p];
+    const uint8_t region = p < h->n_c ? 0 : 1;
+    if (d == 0) {
+      // isolated vertices need no work; they only end a segment
+      close();
+      continue;
+    }
+    const uint8_t b = bucket_of(d);
+    if (open && (cur.bucket != b || cur.region != region || cur.end - cur.begin >= kSegPositions[b] ||
+                 cur.arcs + d > kSegArcs)) {
+      close();
+    }
+    if (!open) {
+      cur = SegInfo{uint32_t(p), uint32_t(p), b, region, 0, 0, 0, 0};
+      open = true;
+    }
+    cur.end = uint32_t(p + 1);
+    cur.max_deg = std::max(cur.max_deg, d);
+    cur.arcs += d;
+  }
+  close();
+}
+
+static void upload_lists(lpa_handle *h) {
+  std::vector<uint32_t> lists[kNumLists];
+  for (size_t s = 0; s < h->segs.size(); s++) {
+    const int v = h->variant[s];
+    const SegInfo &si = h->segs[s];
+    switch (v) {
+      case LPA_VARIANT_WARP:
+        lists[kListWarp].push_back(uint32_t(s));
+        break;
+      case LPA_VARIANT_PACKED:
+        lists[kListPacked].push_back(uint32_t(s));
+        break;
+      case LPA_VARIANT_BLOCK:
+        lists[kListBlock].push_back(uint32_t(s));
+        break;
+      default:
+        if (variant_capable(LPA_VARIANT_WARP, si, h->opts.cms_threshold))
+          lists[kListTwoLight].push_back(uint32_t(s));
+        else
+          lists[kListTwoHeavy].push_back(uint32_t(s));
+    }
+  }
+  std::vector<uint32_t> all;
+  for (int l = 0; l < kNumLists; l++) {
+    h->list_off[l] = uint32_t(all.size());
+    all.insert(all.end(), lists[l].begin(), lists[l].end());
+  }
+  h->list_off[kNumLists] = uint32_t(all.size());
+  h->v4_all_off = h->list_off[kListTwoLight];
+  h->v4_all_n = h->list_off[kListTwoHeavy + 1] - h->list_off[kListTwoLight];
+  if (!h->d_lists) h->d_lists = dalloc<uint32_t>(h, h->segs.size() + 1, "segment lists");
+  h2d(h, h->d_lists, all.data(), all.size(), "upload segment lists");
+  check(h, cudaStreamSynchronize(h->stream), "upload segment lists");
+  h->plan_version++;
+
+  auto grid_for = [&](uint32_t nlist, int occ) {
+    return int(std::max<uint64_t>(1, std::min<uint64_t>(nlist, uint64_t(h->num_sms) * uint64_t(occ))));
+  };
+  h->grid[kListWarp] = grid_for(h->list_off[kListWarp + 1] - h->list_off[kListWarp], h->occ_warp);
+  h->grid[kListPacked] = grid_for(h->list_off[kListPacked + 1] - h->list_off[kListPacked], h->occ_packed);
+  h->grid[kListBlock] = grid_for(h->list_off[kListBlock + 1] - h->list_off[kListBlock], h->occ_block);
+  h->grid[kListTwoLight] = grid_for(h->list_off[kListTwoLight + 1] - h->list_off[kListTwoLight], h->occ_warp);
+  h->grid[kListTwoHeavy] = grid_for(h->list_off[kListTwoHeavy + 1] - h->list_off[kListTwoHeavy], h->occ_block);
+  h->grid_decode = grid_for(h->v4_all_n, 8);
+  if (h->gtab_slots) {
+    h->grid[kListBlock] = std::min(h->grid[kListBlock], h->gtab_blocks);
+    h->grid[kListTwoHeavy] = std::min(h->grid[kListTwoHeavy], h->gtab_blocks);
+  }
+}
+
+static void ensure_two_pass_scratch(lpa_handle *h) {
+  if (h->d_scratch) return;
+  std::vector<uint64_t> off(h->n + 1, 0);
+  for (uint64_t p = 0; p < h->n; p++) off[p + 1] = off[p] + h->h_deg[p];
+  h->d_arc_off = dalloc<uint64_t>(h, h->n + 1, "arc offsets");
+  h2d(h, h->d_arc_off, off.data(), h->n + 1, "upload arc offsets");
+  h->d_scratch = dalloc<uint32_t>(h, off[h->n_c], "two-pass scratch");
+  check(h, cudaStreamSynchronize(h->stream), "arc offsets");
+}
+
+static void apply_dispatch(lpa_handle *h, int dispatch, int force) {
+  h->variant.resize(h->segs.size());
+  bool any_two = false;
+  for (size_t s = 0; s < h->segs.size(); s++) {
+    int v = h->fixed[s];
+    if (dispatch == LPA_DISPATCH_FORCE && variant_capable(force, h->segs[s], h->opts.cms_threshold)) v = force;
+    h->variant[s] = uint8_t(v);
+    any_two |= v == LPA_VARIANT_TWO_PASS;
+  }
+  if (any_two) ensure_two_pass_scratch(h);
+  upload_lists(h);
+}
+
+static void build_plan(lpa_handle *h) {
+  // degrees, decoded once on the device (validates the stream as well)
+  h->d_deg = dalloc<uint32_t>(h, h->n, "degrees");
+  {
+    const int threads = 256;
+    const int blocks = int(std::min<uint64_t>((h->n + threads - 1) / threads, uint64_t(h->num_sms) * 16));
+    k_degree_count<<<std::max(blocks, 1), threads, 0, h->stream>>>(dev_graph(h), h->d_deg, h->d_err);
+    check(h, cudaGetLastError(), "degree kernel launch");
+  }
+  lpa_status st = take_device_error(h);
+  if (st != LPA_OK) throw Fail{st, "degree pass: " + h->last_error};
+  h->h_deg.resize(h->n);
+  check(h, cudaMemcpy(h->h_deg.data(), h->d_deg, h->n * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+        "read degrees");
+  h->m = 0;
+  h->max_deg = 0;
+  for (uint64_t p = 0; p < h->n; p++) {
+    h->m += h->h_deg[p];
+    h->max_deg = std::max<uint64_t>(h->max_deg, h->h_deg[p]);
+  }
+  build_segments(h);
+  h->fixed.resize(h->segs.size());
+  for (size_t s = 0; s < h->segs.size(); s++) h->fixed[s] = uint8_t(fixed_variant(h->segs[s]));
+  std::vector<Seg> ds(h->segs.size());
+  for (size_t s = 0; s < h->segs.size(); s++) ds[s] = Seg{h->segs[s].begin, h->segs[s].end};
+  h->d_segs = dalloc<Seg>(h, ds.size(), "segments");
+  h2d(h, h->d_segs, ds.data(), ds.size(), "upload segments");
+  check(h, cudaStreamSynchronize(h->stream), "upload segments");
+  h->d_seg_cycles = dalloc<long long>(h, h->segs.size(), "segment cycles");
+  check(h, cudaMemsetAsync(h->d_seg_cycles, 0, std::max<size_t>(1, h->segs.size()) * sizeof(long long), h->stream),
+        "clear cycles");
+
+  // global exact-count tables for exact vertices above the shared table
+  uint64_t big = 0;
+  for (uint64_t p = 0; p < h->n; p++) {
+    const uint32_t d = h->h_deg[p];
+    const bool cms = h->opts.cms_threshold != 0 && d >= h->opts.cms_threshold;
+    if (!cms && d > kBlockMaxSmemDeg) big = std::max<uint64_t>(big, d);
+  }
+  if (big) {
+    h->gtab_slots = next_pow2_host(2 * big);
+    const uint64_t per_block = uint64_t(h->gtab_slots) * 2 * sizeof(uint32_t);
+    h->gtab_blocks = int(std::max<uint64_t>(
+        1, std::min<uint64_t>(uint64_t(h->num_sms) * h->occ_block, (1ull << 30) / per_block)));
+    h->d_gtab = dalloc<uint32_t>(h, uint64_t(h->gtab_blocks) * 2 * h->gtab_slots, "global count tables");
+    check(h, cudaMemsetAsync(h->d_gtab, 0, uint64_t(h->gtab_blocks) * per_block, h->stream), "clear tables");
+  }
+  apply_dispatch(h, h->opts.dispatch == LPA_DISPATCH_FORCE ? LPA_DISPATCH_FORCE : LPA_DISPATCH_FIXED,
+                 h->opts.force_variant);
+}
+
+static IterArgs iter_args(lpa_handle *h, int list, unsigned long long *changed) {
+  IterArgs a{};
+  a.g = dev_graph(h);
+  a.labs0 = h->d_lab[0];
+  a.labs1 = h->d_lab[1];
+  a.parity0 = uint32_t(h->cur);
+  a.it_dev = h->loop_it;
+  a.changed = changed;
+  a.err = h->d_err;
+  a.segs = h->d_segs;
+  a.seg_list = h->d_lists + h->list_off[list];
+  a.n_list = h->list_off[list + 1] - h->list_off[list];
+  a.seg_cycles = h->opts.record_timings ? h->d_seg_cycles : nullptr;
+  a.cms_thr = h->opts.cms_threshold;
+  for (int r = 0; r < kCmsDepth; r++) a.seeds[r] = h->seeds[r];
+  a.scratch = h->d_scratch;
+  a.arc_off = h->d_arc_off;
+  a.from_scratch = (list == kListTwoLight || list == kListTwoHeavy) ? 1 : 0;
+  a.gtab = h->d_gtab;
+  a.gtab_slots = h->gtab_slots;
+  return a;
+}
+
+constexpr size_t kSmemPacked = size_t(kLaneWarps) * kStage * sizeof(uint32_t);
+constexpr size_t kSmemWarp = size_t(kLaneWarps) * (kStage + 2 * kV1Slots) * sizeof(uint32_t);
+constexpr size_t kSmemBlock = size_t(2) * kBlockSlots * sizeof(uint32_t);
+
+// Enqueues one iteration (no host synchronisation).  Swaps the buffers.
+static void enqueue_iteration(lpa_handle *h, unsigned long long *changed) {
+  const bool timed = h->opts.record_timings && h->events_ready;
+  auto launch = [&](int list, auto body) {
+    if (h->list_off[list + 1] == h->list_off[list]) return;
+    if (timed) cudaEventRecord(h->ev[2 * list], h->stream);
+    body(iter_args(h, list, changed));
+    h->launches++;
+    if (timed) cudaEventRecord(h->ev[2 * list + 1], h->stream);
+  };
+  if (timed) cudaEventRecord(h->ev[2 * kNumLists], h->stream);
+  launch(kListPacked, [&](const IterArgs &a) {
+    k_lane_batch_packed<<<h->grid[kListPacked], kLaneWarps * 32, kSmemPacked, h->stream>>>(a);
+  });
+  launch(kListWarp, [&](const IterArgs &a) {
+    k_lane_batch_warp<<<h->grid[kListWarp], kLaneWarps * 32, kSmemWarp, h->stream>>>(a);
+  });
+  launch(kListBlock, [&](const IterArgs &a) {
+    k_block<<<h->grid[kListBlock], kBlockThreads, kSmemBlock, h->stream>>>(a);
+  });
+  if (h->v4_all_n) {
+    IterArgs a = iter_args(h, kListTwoLight, changed);
+    a.seg_list = h->d_lists + h->v4_all_off;
+    a.n_list = h->v4_all_n;
+    if (timed) cudaEventRecord(h->ev[2 * kListTwoLight], h->stream);
+    k_decode_segments<<<h->grid_decode, 256, 0, h->stream>>>(a);
+    h->launches++;
+    launch(kListTwoLight, [&](const IterArgs &b) {
+      k_lane_batch_warp<<<h->grid[kListTwoLight], kLaneWarps * 32, kSmemWarp, h->stream>>>(b);
+    });
+    launch(kListTwoHeavy, [&](const IterArgs &b) {
+      k_block<<<h->grid[kListTwoHeavy], kBlockThreads, kSmemBlock, h->stream>>>(b);
+    });
+  }
+  if (timed) cudaEventRecord(h->ev[2 * kNumLists + 1], h->stream);
+  h->cur ^= 1;
+}
+
+static void collect_times(lpa_handle *h) {
+  if (!(h->opts.record_timings && h->events_ready)) return;
+  auto ms = [&](int a, int b) {
+    float t = 0;
+    if (cudaEventElapsedTime(&t, h->ev[a], h->ev[b]) != cudaSuccess) {
+      cudaGetLastError();
+      return 0.0;
+    }
+    return double(t);
+  };
+  for (int v = 0; v < 4; v++) h->variant_ms[v] = 0;
+  if (h->list_off[kListWarp + 1] > h->list_off[kListWarp])
+    h->variant_ms[LPA_VARIANT_WARP] = ms(2 * kListWarp, 2 * kListWarp + 1);
+  if (h->list_off[kListPacked + 1] > h->list_off[kListPacked])
+    h->variant_ms[LPA_VARIANT_PACKED] = ms(2 * kListPacked, 2 * kListPacked + 1);
+  if (h->list_off[kListBlock + 1] > h->list_off[kListBlock])
+    h->variant_ms[LPA_VARIANT_BLOCK] = ms(2 * kListBlock, 2 * kListBlock + 1);
+  if (h->v4_all_n) {
+    const int last = (h->list_off[kListTwoHeavy + 1] > h->list_off[kListTwoHeavy]) ? kListTwoHeavy : kListTwoLight;
+    h->variant_ms[LPA_VARIANT_TWO_PASS] = ms(2 * kListTwoLight, 2 * last + 1);
+  }
+  h->last_iter_ms = ms(2 * kNumLists, 2 * kNumLists + 1);
+}
+
+// ------------------------------------------------------------------ C ABI --
+extern "C" {
+
+const char *lpa_status_str(lpa_status s) {
+  switch (s) {
+    case LPA_OK: return "ok";
+    case LPA_ERR_CUDA: return "CUDA error";
+    case LPA_ERR_OOM: return "out of device memory";
+    case LPA_ERR_BAD_STREAM: return "malformed bitstream";
+    case LPA_ERR_TIMEOUT: return "device wait timed out";
+    case LPA_ERR_INVALID_ARG: return "invalid argument";
+    case LPA_ERR_IO: return "file missing or malformed";
+    case LPA_ERR_NO_DEVICE: return "no CUDA device";
+    case LPA_ERR_CAPACITY: return "planned capacity exceeded";
+  }
+  return "unknown status";
+}
+
+const char *lpa_version(void) { return "lpa_b200 0.1 (sm_100a)"; }
+
+void lpa_opts_default(lpa_opts *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->device = 0;
+  o->cms_threshold = 0;
+  o->cms_seed = 1;
+  o->dispatch = LPA_DISPATCH_FIXED;
+  o->force_variant = LPA_VARIANT_BLOCK;
+  o->stream = nullptr;
+  o->record_timings = 0;
+  o->verbose = 0;
+}
+
+lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **out) {
+  if (!g || !out) return LPA_ERR_INVALID_ARG;
+  *out = nullptr;
+  const uint64_t n = g->num_vertices, n_c = g->num_compressed;
+  if (n == 0 || n > 0xFFFFFFFEull || n_c > n || !g->vertices) return LPA_ERR_INVALID_ARG;
+  if (n_c > 0 && (!g->words || !g->offsets)) return LPA_ERR_INVALID_ARG;
+  if (n > n_c && !g->small_offset) return LPA_ERR_INVALID_ARG;
+  if (g->num_small_arcs > 0 && !g->small_graph) return LPA_ERR_INVALID_ARG;
+  // host-side format checks: monotone offsets inside the stream, small CSR sizes
+  if (n_c > 0) {
+    if (g->offsets[0] != 0) return LPA_ERR_BAD_STREAM;
+    for (uint64_t i = 0; i < n_c; i++)
+      if (g->offsets[i + 1] < g->offsets[i]) return LPA_ERR_BAD_STREAM;
+    if ((g->offsets[n_c] + 31) / 32 > g->num_words) return LPA_ERR_BAD_STREAM;
+  }
+  if (n > n_c) {
+    if (g->small_offset[0] != 0 || g->small_offset[n - n_c] != g->num_small_arcs) return LPA_ERR_INVALID_ARG;
+    for (uint64_t i = 0; i < n - n_c; i++)
+      if (g->small_offset[i + 1] < g->small_offset[i]) return LPA_ERR_INVALID_ARG;
+  }
+
+  lpa_handle *h = new (std::nothrow) lpa_handle();
+  if (!h) return LPA_ERR_OOM;
+  if (o) h->opts = *o;
+  else lpa_opts_default(&h->opts);
+  try {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+      cudaGetLastError();
+      delete h;
+      return LPA_ERR_NO_DEVICE;
+    }
+    if (h->opts.device < 0 || h->opts.device >= count) throw Fail{LPA_ERR_INVALID_ARG, "device ordinal"};
+    h->device = h->opts.device;
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    check(h, cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device), "SM count");
+    if (h->opts.stream) {
+      h->stream = static_cast<cudaStream_t>(h->opts.stream);
+    } else {
+      check(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+      h->own_stream = true;
+    }
+    check(h, cudaFuncSetAttribute(k_lane_batch_packed, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemPacked)),
+          "smem attr");
+    check(h, cudaFuncSetAttribute(k_lane_batch_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemWarp)),
+          "smem attr");
+    check(h, cudaFuncSetAttribute(k_block, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBlock)), "smem attr");
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ_packed, k_lane_batch_packed, kLaneWarps * 32,
+                                                           kSmemPacked), "occupancy");
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ_warp, k_lane_batch_warp, kLaneWarps * 32,
+                                                           kSmemWarp), "occupancy");
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ_block, k_block, kBlockThreads, kSmemBlock),
+          "occupancy");
+    h->occ_packed = std::max(1, h->occ_packed);
+    h->occ_warp = std::max(1, h->occ_warp);
+    h->occ_block = std::max(1, h->occ_block);
+
+    h->n = n;
+    h->n_c = n_c;
+    h->nwords = g->num_words;
+    h->m_small = g->num_small_arcs;
+    h->total_bits = n_c ? g->offsets[n_c] : 0;
+    cms_seeds(h->opts.cms_seed, h->seeds);
+
+    // device copies; the stream gets 4 zero words of tail for the 64-bit window
+    const uint64_t wcount = h->nwords + 4;
+    h->d_words = dalloc<uint32_t>(h, wcount, "bitstream");
+    check(h, cudaMemsetAsync(h->d_words, 0, wcount * sizeof(uint32_t), h->stream), "clear bitstream");
+    h2d(h, h->d_words, g->words, h->nwords, "upload bitstream");
+    h->d_offsets = dalloc<uint64_t>(h, n_c + 1, "offsets");
+    if (n_c) h2d(h, h->d_offsets, g->offsets, n_c + 1, "upload offsets");
+    h->d_vertices = dalloc<uint32_t>(h, n, "vertices");
+    h2d(h, h->d_vertices, g->vertices, n, "upload vertices");
+    h->d_small_off = dalloc<uint32_t>(h, n - n_c + 1, "small offsets");
+    if (n > n_c) h2d(h, h->d_small_off, g->small_offset, n - n_c + 1, "upload small offsets");
+    h->d_small_nbr = dalloc<uint32_t>(h, h->m_small, "small neighbours");
+    h2d(h, h->d_small_nbr, g->small_graph, h->m_small, "upload small neighbours");
+    h->d_lab[0] = dalloc<uint32_t>(h, n, "labels");
+    h->d_lab[1] = dalloc<uint32_t>(h, n, "labels");
+    h->changed_slots = kMaxRunSlots;
+    h->d_changed = dalloc<unsigned long long>(h, h->changed_slots, "changed counters");
+    check(h, cudaMemsetAsync(h->d_changed, 0, h->changed_slots * sizeof(unsigned long long), h->stream),
+          "clear counters");
+    h->d_err = dalloc<uint32_t>(h, 1, "error word");
+    check(h, cudaMemsetAsync(h->d_err, 0, sizeof(uint32_t), h->stream), "clear error word");
+    check(h, cudaMallocHost(&h->h_pinned, sizeof(unsigned long long) * 64), "pinned readback");
+    for (auto &e : h->ev) check(h, cudaEventCreate(&e), "events");
+    h->events_ready = true;
+
+    build_plan(h);
+    // per-segment stream bits for the cost model's features
+    for (auto &s : h->segs)
+      if (s.region == 0) s.bits = g->offsets[s.end] - g->offsets[s.begin];
+    check(h, cudaStreamSynchronize(h->stream), "create");
+    lpa_status st = lpa_init_labels(h);
+    if (st != LPA_OK) throw Fail{st, h->last_error};
+  } catch (const Fail &f) {
+    lpa_status st = f.st;
+    std::fprintf(stderr, "lpa_create: %s\n", f.msg.c_str());
+    lpa_destroy(h);
+    return st;
+  }
+  *out = h;
+  return LPA_OK;
+}
+
+lpa_status lpa_destroy(lpa_handle *h) {
+  if (!h) return LPA_ERR_INVALID_ARG;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  lpa_rt_destroy_graph(h);
+  for (void *p : h->allocations) cudaFree(p);
+  h->allocations.clear();
+  if (h->h_pinned) cudaFreeHost(h->h_pinned);
+  for (auto &e : h->ev)
+    if (e) cudaEventDestroy(e);
+  lpa_learner_free(h);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  cudaGetLastError();
+  delete h;
+  return LPA_OK;
+}
+
+lpa_status lpa_get_info(lpa_handle *h, lpa_info *info) {
+  if (!h || !info) return LPA_ERR_INVALID_ARG;
+  std::memset(info, 0, sizeof(*info));
+  info->num_vertices = h->n;
+  info->num_compressed = h->n_c;
+  info->num_arcs = h->m;
+  info->num_small_arcs = h->m_small;
+  info->stream_bits = h->total_bits;
+  info->num_segments = h->segs.size();
+  info->max_degree = h->max_deg;
+  const uint64_t n_s = h->n - h->n_c;
+  // bitstream + 8(n_c+1) offsets + 4 n_c ids + 4(n_s+1) + 4 m_s small CSR
+  // + 4 n degrees + 4 n label reads + 4 n label writes
+  info->bytes_algorithmic = (h->total_bits + 7) / 8 + 8 * (h->n_c + 1) + 4 * h->n_c + 4 * (n_s + 1) +
+                            4 * h->m_small + 12 * h->n;
+  info->device_bytes = h->device_bytes;
+  return LPA_OK;
+}
+
+const char *lpa_last_error(lpa_handle *h) { return h ? h->last_error.c_str() : "null handle"; }
+
+lpa_status lpa_init_labels(lpa_handle *h) {
+  if (!h) return LPA_ERR_INVALID_ARG;
+  try {
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const int blocks = int(std::min<uint64_t>((h->n + 255) / 256, uint64_t(h->num_sms) * 8));
+    k_init_labels<<<std::max(1, blocks), 256, 0, h->stream>>>(h->d_lab[0], h->d_lab[1], h->n);
+    check(h, cudaGetLastError(), "init labels");
+    h->cur = 0;
+    h->iterations = 0;
+    h->history.clear();
+    check(h, cudaStreamSynchronize(h->stream), "init labels");
+  } catch (const Fail &f) {
+    return guard(h, f);
+  }
+  return LPA_OK;
+}
+
+lpa_status lpa_set_labels(lpa_handle *h, const uint32_t *host, size_t n) {
+  if (!h || !host || n != h->n) return LPA_ERR_INVALID_ARG;
+  try {
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    // both buffers: vertices without neighbours are never rewritten
+    check(h, cudaMemcpyAsync(h->d_lab[0], host, n * 4, cudaMemcpyHostToDevice, h->stream), "set labels");
+    check(h, cudaMemcpyAsync(h->d_lab[1], host, n * 4, cudaMemcpyHostToDevice, h->stream), "set labels");
+    check(h, cudaStreamSynchronize(h->stream), "set labels");
+    h->cur = 0;
+    h->iterations = 0;
+    h->history.clear();
+  } catch (const Fail &f) {
+    return guard(h, f);
+  }
+  return LPA_OK;
+}
+
+
+lpa_status lpa_iterate(lpa_handle *h, uint64_t *changed_out) {
+  if (!h) return LPA_ERR_INVALID_ARG;
+  try {
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    lpa_learner_before_iteration(h);
+    unsigned long long *slot = h->d_changed;
+    check(h, cudaMemsetAsync(slot, 0, sizeof(unsigned long long), h->stream), "clear counter");
+    enqueue_iteration(h, slot);
+    check(h, cudaGetLastError(), "iteration launch");
+    check(h, cudaMemcpyAsync(h->h_pinned, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream),
+          "read counter");
+    lpa_status st = take_device_error(h);  // synchronises
+    if (st != LPA_OK) return st;
+    h->last_changed = h->h_pinned[0];
+    h->history.push_back(h->last_changed);
+    h->iterations++;
+    collect_times(h);
+    lpa_learner_after_iteration(h);
+    if (h->opts.verbose)
+      std::printf("%llu: %f (ms), updated %llu\n", (unsigned long long)h->iterations, h->last_iter_ms,
+                  (unsigned long long)h->last_changed);
+    if (changed_out) *changed_out = h->last_changed;
+  } catch (const Fail &f) {
+    return guard(h, f);
+  }
+  return LPA_OK;
+}
+
+
+lpa_status lpa_run(lpa_handle *h, int max_iter, int early_exit, int *iters_done) {
+  if (!h || max_iter < 0) return LPA_ERR_INVALID_ARG;
+  if (iters_done) *iters_done = 0;
+  return lpa_run_graph(h, max_iter, early_exit != 0, iters_done);
+}
+
+lpa_status lpa_get_changed_history(lpa_handle *h, uint64_t *out, size_t count) {
+  if (!h || (!out && count)) return LPA_ERR_INVALID_ARG;
+  if (count > h->history.size()) return LPA_ERR_INVALID_ARG;
+  const size_t base = h->history.size() - count;
+  for (size_t i = 0; i < count; i++) out[i] = h->history[base + i];
+  return LPA_OK;
+}
+
+lpa_status lpa_get_labels(lpa_handle *h, uint32_t *host_out, size_t n) {
+  if (!h || !host_out || n != h->n) return LPA_ERR_INVALID_ARG;
+  try {
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    check(h, cudaMemcpyAsync(host_out, h->d_lab[h->cur], n * 4, cudaMemcpyDeviceToHost, h->stream), "get labels");
+    check(h, cudaStreamSynchronize(h->stream), "get labels");
+  } catch (const Fail &f) {
+    return guard(h, f);
+  }
+  return LPA_OK;
+}
+
+lpa_status lpa_get_stats(lpa_handle *h, lpa_stats *st) {
+  if (!h || !st) return LPA_ERR_INVALID_ARG;
+  std::memset(st, 0, sizeof(*st));
+  st->iterations = h->iterations;
+  st->last_changed = h->last_changed;
+  st->last_iter_ms = h->last_iter_ms;
+  st->launches = h->launches;
+  for (int v = 0; v < 4; v++) st->variant_ms[v] = h->variant_ms[v];
+  for (size_t s = 0; s < h->segs.size(); s++) {
+    st->variant_segments[h->variant[s]]++;
+    st->variant_arcs[h->variant[s]] += h->segs[s].arcs;
+  }
+  lpa_learner_stats(h, st);
+  return LPA_OK;
+}
+
+lpa_status lpa_get_degrees(lpa_handle *h, uint32_t *deg_out, size_t n) {
+  if (!h || !deg_out || n != h->n) return LPA_ERR_INVALID_ARG;
+  std::memcpy(deg_out, h->h_deg.data(), n * sizeof(uint32_t));
+  return LPA_OK;
+}
+
+lpa_status lpa_decode_csr(lpa_handle *h, uint64_t *row_out, uint32_t *clm_out) {
+  if (!h || !row_out || (!clm_out && h->m)) return LPA_ERR_INVALID_ARG;
+  try {
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    ensure_two_pass_scratch(h);
+    DecodeArgs a{};
+    a.g = dev_graph(h);
+    a.pos_list = nullptr;
+    a.n_pos = h->n_c;
+    a.arc_off = h->d_arc_off;
+    a.out = h->d_scratch;
+    a.err = h->d_err;
+    const int blocks = int(std::max<uint64_t>(1, std::min<uint64_t>((h->n_c + 255) / 256, uint64_t(h->num_sms) * 8)));
+    if (h->n_c) k_decode_positions<<<blocks, 256, 0, h->stream>>>(a);
+    check(h, cudaGetLastError(), "decode launch");
+    lpa_status st = take_device_error(h);
+    if (st != LPA_OK) return st;
+    std::vector<uint64_t> off(h->n + 1, 0);
+    for (uint64_t p = 0; p < h->n; p++) off[p + 1] = off[p] + h->h_deg[p];
+    std::vector<uint32_t> ids(off[h->n_c]);
+    std::vector<uint32_t> verts(h->n);
+    check(h, cudaMemcpy(ids.data(), h->d_scratch, ids.size() * 4, cudaMemcpyDeviceToHost), "read decode");
+    check(h, cudaMemcpy(verts.data(), h->d_vertices, h->n * 4, cudaMemcpyDeviceToHost), "read vertices");
+    std::vector<uint32_t> sm_off(h->n - h->n_c + 1, 0), sm_nbr(h->m_small);
+    if (h->n > h->n_c)
+      check(h, cudaMemcpy(sm_off.data(), h->d_small_off, sm_off.size() * 4, cudaMemcpyDeviceToHost), "read small");
+    if (h->m_small)
+      check(h, cudaMemcpy(sm_nbr.data(), h->d_small_nbr, sm_nbr.size() * 4, cudaMemcpyDeviceToHost), "read small");
+    std::vector<uint64_t> deg_by_id(h->n + 1, 0);
+    for (uint64_t p = 0; p < h->n; p++) deg_by_id[verts[p]] = h->h_deg[p];
+    row_out[0] = 0;
+    for (uint64_t v = 0; v < h->n; v++) row_out[v + 1] = row_out[v] + deg_by_id[v];
+    for (uint64_t p = 0; p < h->n; p++) {
+      const uint32_t v = verts[p];
+      const uint32_t *src = p < h->n_c ? ids.data() + off[p] : sm_nbr.data() + sm_off[p - h->n_c];
+      std::memcpy(clm_out + row_out[v], src, size_t(h->h_deg[p]) * 4);
+    }
+  } catch (const Fail &f) {
+    return guard(h, f);
+  }
+  return LPA_OK;
+}
+
+lpa_status lpa_set_dispatch(lpa_handle *h, int dispatch, int force_variant) {
+  if (!h || dispatch < 0 || dispatch > 2 || force_variant < 0 || force_variant > 3) return LPA_ERR_INVALID_ARG;
+  try {
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    h->opts.dispatch = dispatch;
+    h->opts.force_variant = force_variant;
+    lpa_learner_reset(h);
+    apply_dispatch(h, dispatch == LPA_DISPATCH_FORCE ? LPA_DISPATCH_FORCE : LPA_DISPATCH_FIXED, force_variant);
+    check(h, cudaStreamSynchronize(h->stream), "dispatch");
+  } catch (const Fail &f) {
+    return guard(h, f);
+  }
+  return LPA_OK;
+}
+
+lpa_status lpa_get_segments(lpa_handle *h, uint32_t *begin, uint32_t *end, uint8_t *bucket, uint8_t *variant,
+                            size_t count) {
+  if (!h || count != h->segs.size()) return LPA_ERR_INVALID_ARG;
+  for (size_t s = 0; s < count; s++) {
+    if (begin) begin[s] = h->segs[s].begin;
+    if (end) end[s] = h->segs[s].end;
+    if (bucket) bucket[s] = h->segs[s].bucket;
+    if (variant) variant[s] = h->variant[s];
+  }
+  return LPA_OK;
+}
+
+}  // extern "C"
+
+// Internal hooks used by the dispatch and graph-loop modules.
+void lpa_rt_enqueue_iteration(lpa_handle *h, unsigned long long *changed) { enqueue_iteration(h, changed); }
+void lpa_rt_apply_variants(lpa_handle *h) {
+  bool any_two = false;
+  for (auto v : h->variant) any_two |= v == LPA_VARIANT_TWO_PASS;
+  if (any_two) ensure_two_pass_scratch(h);
+  upload_lists(h);
+}
+lpa_status lpa_rt_take_error(lpa_handle *h) { return take_device_error(h); }

@@ -1,0 +1,127 @@
+// Internal runtime structures behind the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "lp_kernels.cuh"
+#include "lpa_capi.h"
+
+namespace lpa_rt {
+
+// Degree buckets used to cut segments (the reference's buckets,
+// baselines/novaplus/novaplus_propogator.cuh:219-220, plus a "heavy" bucket
+// for vertices only the block and two-pass variants can take).
+enum Bucket : uint8_t { kTiny = 0, kMid = 1, kLarge = 2, kHeavy = 3, kNumBuckets = 4 };
+
+// Launch lists: one per variant, the two-pass variant split by the kernel
+// that counts its segments.
+enum List : int { kListWarp = 0, kListPacked = 1, kListBlock = 2, kListTwoLight = 3, kListTwoHeavy = 4,
+                  kNumLists = 5 };
+
+struct SegInfo {
+  uint32_t begin, end;
+  uint8_t bucket;
+  uint8_t region;  // 0: compressed, 1: small CSR
+  uint32_t max_deg;
+  uint64_t arcs;
+  uint64_t bits;
+  uint32_t intervals;  // interval count (features)
+};
+
+struct CudaError {
+  cudaError_t e;
+  const char *where;
+};
+
+inline uint32_t next_pow2_host(uint64_t x) {
+  uint32_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+bool variant_capable(int variant, const SegInfo &s, uint32_t cms_thr);
+int fixed_variant(const SegInfo &s);
+
+}  // namespace lpa_rt
+
+struct lpa_handle {
+  lpa_opts opts{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string last_error;
+  int num_sms = 148;
+
+  uint64_t n = 0, n_c = 0, nwords = 0, m_small = 0, m = 0, total_bits = 0, max_deg = 0;
+  uint32_t seeds[lpa_dev::kCmsDepth] = {0, 0, 0, 0};
+
+  // device graph
+  uint32_t *d_words = nullptr, *d_vertices = nullptr, *d_deg = nullptr;
+  uint32_t *d_small_off = nullptr, *d_small_nbr = nullptr;
+  uint64_t *d_offsets = nullptr;
+  uint32_t *d_lab[2] = {nullptr, nullptr};
+  int cur = 0;
+  unsigned long long *d_changed = nullptr;  // one slot per iteration of a run
+  int changed_slots = 0;
+  uint32_t *d_err = nullptr;
+  unsigned long long *h_pinned = nullptr;  // pinned readback
+
+  // plan
+  std::vector<uint32_t> h_deg;
+  std::vector<lpa_rt::SegInfo> segs;
+  std::vector<uint8_t> variant;  // per segment
+  std::vector<uint8_t> fixed;    // per segment, the heuristic's choice
+  lpa_dev::Seg *d_segs = nullptr;
+  uint32_t *d_lists = nullptr;
+  uint32_t list_off[lpa_rt::kNumLists + 1] = {0};
+  uint32_t v4_all_off = 0, v4_all_n = 0;  // two-pass segments (both lists) for pass 1
+  int grid[lpa_rt::kNumLists] = {0};
+  int grid_decode = 0;
+  int occ_packed = 1, occ_warp = 1, occ_block = 1;
+
+  // scratch
+  uint64_t *d_arc_off = nullptr;
+  uint32_t *d_scratch = nullptr;
+  uint32_t *d_gtab = nullptr;
+  uint32_t gtab_slots = 0;
+  int gtab_blocks = 0;
+  long long *d_seg_cycles = nullptr;
+
+  // stats
+  uint64_t iterations = 0;
+  uint64_t launches = 0;
+  uint64_t last_changed = 0;
+  std::vector<uint64_t> history;
+  double last_iter_ms = 0;
+  double variant_ms[4] = {0, 0, 0, 0};
+  cudaEvent_t ev[2 * lpa_rt::kNumLists + 2] = {};
+  bool events_ready = false;
+  uint64_t device_bytes = 0;
+  std::vector<void *> allocations;
+
+  // CUDA-graph loop: while set, kernels take their parity and counter slot from it
+  const uint32_t *loop_it = nullptr;
+  uint32_t *d_loop_it = nullptr;
+  void *graph_exec = nullptr;  // cudaGraphExec_t of the early-exit loop
+  void *graph = nullptr;       // cudaGraph_t
+  uint64_t launches_per_graph_iteration = 0;
+  uint64_t plan_version = 0, graph_plan_version = ~0ull;
+
+  // learned dispatch (cost model), see dispatch.cu
+  struct Learner *learner = nullptr;
+};
+
+// Hooks between the runtime modules (C++ linkage).
+void lpa_rt_destroy_graph(lpa_handle *h);
+lpa_status lpa_run_graph(lpa_handle *h, int max_iter, bool early_exit, int *iters_done);
+void lpa_learner_free(lpa_handle *h);
+void lpa_learner_reset(lpa_handle *h);
+void lpa_learner_before_iteration(lpa_handle *h);
+void lpa_learner_after_iteration(lpa_handle *h);
+void lpa_learner_stats(lpa_handle *h, lpa_stats *st);
+void lpa_rt_enqueue_iteration(lpa_handle *h, unsigned long long *changed);
+void lpa_rt_apply_variants(lpa_handle *h);
+lpa_status lpa_rt_take_error(lpa_handle *h);
