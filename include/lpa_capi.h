@@ -31,6 +31,9 @@
 extern "C" {
 #endif
 
+typedef struct lpa_handle lpa_handle; /* one device-resident graph (propagator) */
+typedef struct lpa_batch lpa_batch;   /* many graphs propagated together */
+
 typedef enum lpa_status {
   LPA_OK = 0,
   LPA_ERR_CUDA = 1,        /* a CUDA runtime call failed */
@@ -79,7 +82,7 @@ typedef struct lpa_opts {
   int dispatch;            /* lpa_dispatch */
   int force_variant;       /* lpa_variant, with LPA_DISPATCH_FORCE */
   void *stream;            /* cudaStream_t to run on; NULL: the handle makes one */
-  int record_timings;      /* per-segment device cycles and per-launch events */
+  int record_timings;      /* 1: per-launch events; 2: also per-segment device cycles */
   int verbose;             /* per-iteration log lines on stdout */
 } lpa_opts;
 
@@ -104,6 +107,8 @@ typedef struct lpa_stats {
   uint64_t dispatch_reverts;        /* times the learned plan was judged slower */
   int learned_active;               /* 1 when the learned plan is in use */
   uint64_t launches;                /* kernel launches enqueued by this handle */
+  double decode_ms;                 /* two-pass decode kernel, last iteration */
+  double iterate_ms;                /* persistent iteration kernel, last iteration */
 } lpa_stats;
 
 /* ---------------------------------------------------------------- basics -- */
@@ -156,6 +161,24 @@ lpa_status lpa_set_dispatch(struct lpa_handle *h, int dispatch, int force_varian
 /* Per-segment view of the plan: begin/end positions, bucket, variant. */
 lpa_status lpa_get_segments(struct lpa_handle *h, uint32_t *begin, uint32_t *end, uint8_t *bucket,
                             uint8_t *variant, size_t count);
+
+/* ------------------------------------------------ dispatch cost model ---- */
+/* The 6 -> 32 -> 32 -> 4 fp32 MLP behind LPA_DISPATCH_LEARNED (no reference
+ * counterpart; the reference dispatches by fixed degree buckets only).
+ * Parameters are 1412 floats: W1[32][6] b1[32] W2[32][32] b2[32] W3[4][32] b3[4]. */
+#define LPA_MLP_PARAMS 1412
+/* Gradient (1412 floats) of sum_k 0.5 (y_k[variant_k] - target_k)^2 over n
+ * samples x (n x 6), computed by the library's own backward kernel. */
+lpa_status lpa_mlp_gradient(int device, const float *params, const float *x, const uint8_t *variant,
+                            const float *target, size_t n, float *grad_out, float *loss_out);
+/* Forward pass on the device: out receives n x 4 predicted log-costs. */
+lpa_status lpa_mlp_predict(int device, const float *params, const float *x, size_t n, float *out);
+/* The handle's current parameters (the initial ones before any training). */
+lpa_status lpa_get_mlp(struct lpa_handle *h, float *params, size_t n);
+/* The last learned plan (variant per segment) and its predictions (4 per segment). */
+lpa_status lpa_get_learned_plan(struct lpa_handle *h, uint8_t *plan, float *pred, size_t count);
+/* Device cycles per segment of the last iteration that recorded them. */
+lpa_status lpa_get_segment_cycles(struct lpa_handle *h, uint64_t *cycles, size_t count);
 
 /* ------------------------------------------ host format layer (lpa_hg_*) --- */
 /* A host graph owns a CSR (by vertex id) and/or its compressed form, produced

@@ -118,6 +118,8 @@ class Stats(C.Structure):
         ("dispatch_reverts", C.c_uint64),
         ("learned_active", C.c_int),
         ("launches", C.c_uint64),
+        ("decode_ms", C.c_double),
+        ("iterate_ms", C.c_double),
     ]
 
 
@@ -170,6 +172,12 @@ def lib():
     _sig(L, "lpa_hg_csr", [P, u64p, C.POINTER(u64p), C.POINTER(u32p)])
     _sig(L, "lpa_hg_desc", [P, C.POINTER(GraphDesc)])
     _sig(L, "lpa_hg_free", [P])
+    fp = C.POINTER(C.c_float)
+    _sig(L, "lpa_mlp_gradient", [C.c_int, fp, fp, u8p, fp, C.c_size_t, fp, fp])
+    _sig(L, "lpa_mlp_predict", [C.c_int, fp, fp, C.c_size_t, fp])
+    _sig(L, "lpa_get_mlp", [P, fp, C.c_size_t])
+    _sig(L, "lpa_get_learned_plan", [P, u8p, fp, C.c_size_t])
+    _sig(L, "lpa_get_segment_cycles", [P, u64p, C.c_size_t])
     _sig(L, "lpa_batch_create", [C.POINTER(GraphDesc), C.c_size_t, C.POINTER(Opts), PP])
     _sig(L, "lpa_batch_run", [P, C.c_int, C.c_int, u32p])
     _sig(L, "lpa_batch_get_labels", [P, C.c_size_t, u32p, C.c_size_t])
@@ -403,6 +411,25 @@ class Propagator:
     def set_dispatch(self, dispatch, force_variant=Variant.BLOCK):
         self._chk(lib().lpa_set_dispatch(self._h, int(dispatch), int(force_variant)), "lpa_set_dispatch")
 
+    def mlp_params(self) -> np.ndarray:
+        out = np.zeros(MLP_PARAMS, np.float32)
+        self._chk(lib().lpa_get_mlp(self._h, _ptr(out, C.c_float), MLP_PARAMS), "lpa_get_mlp")
+        return out
+
+    def learned_plan(self):
+        k = int(self.get_info().num_segments)
+        plan = np.zeros(k, np.uint8)
+        pred = np.zeros((k, 4), np.float32)
+        self._chk(lib().lpa_get_learned_plan(self._h, _ptr(plan, C.c_uint8), _ptr(pred, C.c_float), k),
+                  "lpa_get_learned_plan")
+        return plan, pred
+
+    def segment_cycles(self) -> np.ndarray:
+        k = int(self.get_info().num_segments)
+        out = np.zeros(k, np.uint64)
+        self._chk(lib().lpa_get_segment_cycles(self._h, _ptr(out, C.c_uint64), k), "lpa_get_segment_cycles")
+        return out
+
     def segments(self):
         k = int(self.get_info().num_segments)
         b = np.empty(k, np.uint32)
@@ -412,6 +439,31 @@ class Propagator:
         self._chk(lib().lpa_get_segments(self._h, _ptr(b, C.c_uint32), _ptr(e, C.c_uint32), _ptr(bk, C.c_uint8),
                                          _ptr(v, C.c_uint8), k), "lpa_get_segments")
         return b, e, bk, v
+
+
+MLP_PARAMS = 1412
+
+
+def mlp_gradient(params, x, variant, target, device=0):
+    """Gradient of the dispatch cost model, computed by the library's GPU kernel."""
+    P = np.ascontiguousarray(params, np.float32)
+    X = np.ascontiguousarray(x, np.float32)
+    V = np.ascontiguousarray(variant, np.uint8)
+    T = np.ascontiguousarray(target, np.float32)
+    g = np.zeros(MLP_PARAMS, np.float32)
+    loss = C.c_float()
+    _check(lib().lpa_mlp_gradient(device, _ptr(P, C.c_float), _ptr(X, C.c_float), _ptr(V, C.c_uint8),
+                                  _ptr(T, C.c_float), len(T), _ptr(g, C.c_float), C.byref(loss)), "lpa_mlp_gradient")
+    return g, float(loss.value)
+
+
+def mlp_predict(params, x, device=0):
+    P = np.ascontiguousarray(params, np.float32)
+    X = np.ascontiguousarray(x, np.float32)
+    out = np.zeros((len(X), 4), np.float32)
+    _check(lib().lpa_mlp_predict(device, _ptr(P, C.c_float), _ptr(X, C.c_float), len(X), _ptr(out, C.c_float)),
+           "lpa_mlp_predict")
+    return out
 
 
 class LabelPropagator:

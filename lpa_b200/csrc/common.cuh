@@ -170,6 +170,135 @@ __device__ __forceinline__ int64_t walk_vertex(W w, uint64_t pos, uint64_t end, 
   return cnt_all;
 }
 
+// Sequential MSB-first reader with a 64-bit register buffer: one 32-bit load
+// per 32 bits consumed.  Codes that do not fit the buffer's fast path (gamma
+// with >= 16 leading zeros, zeta with >= 8) are read through win64.
+struct BitReader {
+  const uint32_t *__restrict__ w;
+  uint64_t pos;    // absolute position of the next unread bit
+  uint64_t buf;    // upcoming bits, MSB-aligned
+  uint64_t wnext;  // next word to load into buf
+  uint32_t nb;     // valid bits in buf
+
+  __device__ __forceinline__ void seek(const uint32_t *__restrict__ words, uint64_t p) {
+    w = words;
+    pos = p;
+    const uint64_t i = p >> 5;
+    const uint32_t s = uint32_t(p) & 31u;
+    const uint64_t a = __ldg(w + i), b = __ldg(w + i + 1);
+    buf = ((a << 32) | b) << s;
+    nb = 64 - s;
+    wnext = i + 2;
+  }
+  __device__ __forceinline__ void fill() {
+    if (nb <= 32) {
+      buf |= uint64_t(__ldg(w + wnext)) << (32 - nb);
+      wnext++;
+      nb += 32;
+    }
+  }
+  __device__ __forceinline__ void skip(uint32_t k) {  // k < 64, k <= nb
+    buf <<= k;
+    nb -= k;
+    pos += k;
+  }
+  __device__ __forceinline__ uint32_t gamma(bool &bad) {
+    fill();
+    const uint32_t z = __clzll(buf);
+    if (z < 16) {  // 2z+1 <= 31 bits, and nb >= 33 after fill
+      const uint32_t len = 2 * z + 1;
+      const uint32_t v = uint32_t(buf >> (64 - len));
+      skip(len);
+      return v - 1u;
+    }
+    uint64_t p = pos;
+    const uint32_t v = dec_gamma(GWords{w}, p, bad);
+    seek(w, p);
+    return v;
+  }
+  __device__ __forceinline__ uint32_t zeta3(bool &bad) {
+    fill();
+    const uint32_t h = __clzll(buf);
+    if (h < 8) {  // 4(h+1) <= 32 bits
+      const uint32_t v = uint32_t((buf << (h + 1)) >> (64 - 3 * (h + 1)));
+      skip(4 * (h + 1));
+      return v - 1u;
+    }
+    uint64_t p = pos;
+    const uint32_t v = dec_zeta3(GWords{w}, p, bad);
+    seek(w, p);
+    return v;
+  }
+  __device__ __forceinline__ uint32_t segcnt(bool &bad) {
+    fill();
+    const uint32_t z = __clzll(buf);
+    if (z == 0) {
+      if ((buf >> 62) & 1ull) {
+        skip(2);
+        return 0;
+      }
+      skip(1);
+      return 1;
+    }
+    return gamma(bad) + 1u;
+  }
+};
+
+// Walks one vertex with the buffered reader (same contract as walk_vertex).
+template <class Emit>
+__device__ __forceinline__ int64_t walk_vertex_buf(const uint32_t *__restrict__ words, uint64_t pos, uint64_t end,
+                                                   uint32_t node, uint64_t n, Emit emit,
+                                                   int64_t *interval_items = nullptr) {
+  bool bad = false;
+  int64_t cnt_all = 0;
+  BitReader r;
+  r.seek(words, pos);
+  uint32_t nseg = r.segcnt(bad);
+  const uint64_t ibase = r.pos;
+  uint64_t last = r.pos;
+  if (bad || r.pos > end || nseg > (end - r.pos) / kSegBits + 1) return -1;
+  for (uint32_t j = 0; j < nseg; j++) {
+    const uint64_t q = ibase + uint64_t(kSegBits) * j;
+    if (q >= end) return -1;
+    if (j) r.seek(words, q);
+    const uint32_t cnt = r.gamma(bad);
+    uint32_t left = 0;
+    for (uint32_t c = 0; c < cnt; c++) {
+      const uint32_t l = r.gamma(bad);
+      left = (c == 0) ? zigzag_first(node, l) : left + l + 1u;
+      const uint32_t len = r.gamma(bad) + kMinItv;
+      if (bad || r.pos > end || uint64_t(left) + len > n) return -1;
+      for (uint32_t k = 0; k < len; k++) emit(left + k);
+      cnt_all += len;
+      left += len;
+    }
+    last = r.pos;
+  }
+  if (interval_items) *interval_items = cnt_all;
+  r.seek(words, last);
+  nseg = r.segcnt(bad);
+  const uint64_t rbase = r.pos;
+  last = r.pos;
+  if (bad || r.pos > end || nseg > (end - r.pos) / kSegBits + 1) return -1;
+  for (uint32_t j = 0; j < nseg; j++) {
+    const uint64_t q = rbase + uint64_t(kSegBits) * j;
+    if (q >= end) return -1;
+    if (j) r.seek(words, q);
+    const uint32_t cnt = r.gamma(bad);
+    uint32_t v = 0;
+    for (uint32_t c = 0; c < cnt; c++) {
+      const uint32_t x = r.zeta3(bad);
+      v = (c == 0) ? zigzag_first(node, x) : v + x + 1u;
+      if (bad || r.pos > end || uint64_t(v) >= n) return -1;
+      emit(v);
+      cnt_all++;
+    }
+    last = r.pos;
+  }
+  if (bad || last != end) return -1;
+  return cnt_all;
+}
+
 // ---------------------------------------------------------------- hashing --
 // Count-min-sketch row hashes, include/cms.cuh:96-132 (cm_hash1..cm_hash4).
 __device__ __forceinline__ uint32_t cm_hash(int r, uint32_t k) {

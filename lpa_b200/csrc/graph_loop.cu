@@ -65,7 +65,7 @@ cudaError_t build_graph(lpa_handle *h) {
   h->opts.record_timings = 0;
   h->loop_it = h->d_loop_it;
   const uint64_t launches = h->launches;
-  lpa_rt_enqueue_iteration(h, h->d_changed);
+  lpa_rt_enqueue_iteration(h, h->d_changed, h->d_work);
   h->launches_per_graph_iteration = h->launches - launches + 1;
   h->launches = launches;
   k_loop_step<<<1, 1, 0, h->stream>>>(h->d_loop_it, h->d_changed, cond);
@@ -123,6 +123,8 @@ lpa_status lpa_run_graph(lpa_handle *h, int max_iter, bool early_exit, int *iter
   ctl[2] = early_exit ? 1u : 0u;
   e = cudaMemsetAsync(h->d_changed, 0, size_t(max_iter + 2) * sizeof(unsigned long long), h->stream);
   if (e != cudaSuccess) return fail(e, "clear counters");
+  e = cudaMemsetAsync(h->d_work, 0, size_t(2 * (max_iter + 2)) * sizeof(uint32_t), h->stream);
+  if (e != cudaSuccess) return fail(e, "clear work counters");
   e = cudaMemcpyAsync(h->d_loop_it, ctl, 3 * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream);
   if (e != cudaSuccess) return fail(e, "loop control");
   e = cudaGraphLaunch(static_cast<cudaGraphExec_t>(h->graph_exec), h->stream);

@@ -7,15 +7,41 @@
 // seeded cm_hash rows (include/cms.cuh:96-132) and take the argmax of the
 // sketch estimate over their neighbour labels, smallest label on ties.
 //
-// Work is organised in segments: contiguous ranges of positions (the
-// vertices[] order of the compressed graph).  Each launch handles a list of
-// segments; a block takes one segment at a time.
+// k_iterate is a persistent kernel fed by two device work queues:
+//   * heavy items (block variant, and two-pass segments above the warp
+//     limit), taken by a whole block, largest first: 256-bit segments decode in
+//     parallel (one thread each), ids are staged in shared memory, labels are
+//     gathered with many loads in flight, then counted in a shared (or global)
+//     table or the sketch;
+//   * light chunks of up to 32 consecutive positions, taken by one warp: each
+//     lane decodes one vertex into the warp's staging area, the warp gathers
+//     all labels at once, then counts per vertex (one vertex per round, or
+//     several vertices per round for degrees <= 32).
+// Every loop is bounded by the bits it consumes; malformed input sets the
+// error word instead of trapping.
 #include "lp_kernels.cuh"
 
 namespace lpa_dev {
 
-__device__ __forceinline__ uint32_t next_pow2(uint32_t x) {
-  return x <= 1 ? 1u : (1u << (32 - __clz(x - 1)));
+namespace {
+
+__device__ __forceinline__ uint32_t next_pow2(uint32_t x) { return x <= 1 ? 1u : (1u << (32 - __clz(x - 1))); }
+
+struct Ctx {
+  const uint32_t *lab_in;
+  uint32_t *lab_out;
+  unsigned long long *changed;
+  uint32_t it;
+};
+
+__device__ __forceinline__ Ctx resolve(const IterArgs &a) {
+  Ctx c;
+  c.it = iter_index(a);
+  const uint32_t par = (a.parity0 + c.it) & 1u;
+  c.lab_in = par ? a.labs1 : a.labs0;
+  c.lab_out = par ? a.labs0 : a.labs1;
+  c.changed = a.changed + (a.it_dev ? c.it : 0u);
+  return c;
 }
 
 __device__ __forceinline__ void flush_changed(unsigned long long *counter, unsigned long long mine) {
@@ -24,447 +50,584 @@ __device__ __forceinline__ void flush_changed(unsigned long long *counter, unsig
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(counter, mine);
 }
 
-// ---------------------------------------------------------------------------
-// V1 / V2: lane-per-vertex decode into a per-warp staging buffer, then count.
-// ---------------------------------------------------------------------------
-template <bool kPacked>
-__device__ __forceinline__ void lane_batch(const IterArgs &a) {
-  extern __shared__ uint32_t smem[];
-  const int warp = threadIdx.x >> 5;
-  const uint32_t lane = threadIdx.x & 31u;
-  uint32_t *stage = smem + warp * kStage;
-  uint32_t *keys = smem + kLaneWarps * kStage + warp * (2 * kV1Slots);
-  uint32_t *cnts = keys + kV1Slots;
-  const DevGraph &g = a.g;
-  const uint32_t *lab_in;
-  uint32_t *lab_out;
-  unsigned long long *counter;
-  resolve_iter(a, lab_in, lab_out, counter);
-  unsigned long long changed = 0;
-  if (!kPacked) {  // tables start empty and are cleared after every vertex
-    for (uint32_t i = lane; i < 2 * kV1Slots; i += 32) keys[i] = 0u;
-    __syncwarp();
-  }
-
-  for (uint32_t li = blockIdx.x; li < a.n_list; li += gridDim.x) {
-    const uint32_t s = a.seg_list[li];
-    const Seg seg = a.segs[s];
-    const long long t0 = clock64();
-    const uint32_t nchunks = (seg.end - seg.begin + 31) / 32;
-    for (uint32_t c = warp; c < nchunks; c += kLaneWarps) {
-      const uint32_t p = seg.begin + c * 32 + lane;
-      const bool valid = p < seg.end;
-      const uint32_t node = valid ? g.vertices[p] : 0u;
-      uint32_t d = valid ? g.deg[p] : 0u;
-      const uint32_t old = valid ? __ldg(lab_in + node) : 0u;
-      const bool cgr = valid && p < g.n_c;
-      const uint32_t *items = nullptr;
-      if (valid && !cgr) items = g.small_nbr + g.small_off[p - g.n_c];
-      else if (cgr && a.from_scratch) items = a.scratch + a.arc_off[p];
-      const bool need_stage = cgr && !a.from_scratch;
-      if (kPacked ? d > kV2MaxDeg : d > kV1MaxDeg) {
-        set_error(a.err, kErrCapacity);
-        d = 0;
-      }
-
-      uint32_t done = ~__ballot_sync(kFull, valid);
-      while (done != kFull) {
-        const bool pending = !((done >> lane) & 1u);
-        const uint32_t sd = (pending && need_stage) ? d : 0u;
-        uint32_t incl = sd;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          uint32_t t = __shfl_up_sync(kFull, incl, o);
-          if (lane >= uint32_t(o)) incl += t;
-        }
-        const bool in_batch = pending && incl <= kStage;
-        const uint32_t batch = __ballot_sync(kFull, in_batch);
-        if (in_batch && need_stage) {
-          const uint32_t base = incl - sd;
-          uint32_t k = 0;
-          const int64_t r = walk_vertex(GWords{g.words}, g.offsets[p], g.offsets[p + 1], node, g.n,
-                                        [&](uint32_t id) {
-                                          if (k < d) stage[base + k] = id;
-                                          k++;
-                                        });
-          if (r != int64_t(d)) {
-            set_error(a.err, kErrBadStream);
-            for (uint32_t q = (r > 0 ? uint32_t(r) : 0u); q < d; q++) stage[base + q] = node;
-          }
-          items = stage + base;
-        }
-        __syncwarp();
-        if (batch) {
-          const uint32_t lo = __ffs(batch) - 1, hi = 32 - __clz(batch);
-          if (kPacked) {
-            // several vertices per round: G lanes per vertex
-            const uint32_t dmax = __reduce_max_sync(kFull, ((batch >> lane) & 1u) ? d : 0u);
-            const uint32_t G = next_pow2(dmax);
-            const uint32_t per = 32 / G;
-            const uint32_t gl = lane / G, k = lane % G;
-            const uint32_t gm = (G == 32) ? kFull : (((1u << G) - 1u) << (gl * G));
-            for (uint32_t v0 = lo; v0 < hi; v0 += per) {
-              const uint32_t vi = v0 + gl;
-              const bool vin = vi < hi;
-              const uint32_t src = vin ? vi : lo;
-              const uint32_t dv = __shfl_sync(kFull, d, src);
-              const uint32_t *ip =
-                  reinterpret_cast<const uint32_t *>(__shfl_sync(kFull, (unsigned long long)items, src));
-              const uint32_t nodev = __shfl_sync(kFull, node, src);
-              const uint32_t oldv = __shfl_sync(kFull, old, src);
-              const bool ok = vin && k < dv;
-              const uint32_t lab = ok ? __ldg(lab_in + ip[k]) : kFull;
-              const uint32_t m = __match_any_sync(kFull, (uint64_t(gl) << 32) | lab);
-              const uint32_t cnt = ok ? __popc(m) : 0u;
-              const uint32_t maxc = __reduce_max_sync(gm, cnt);
-              const uint32_t best = __reduce_min_sync(gm, (ok && cnt == maxc) ? lab : kFull);
-              if (vin && k == 0) {
-                const uint32_t nl = dv ? best : oldv;
-                lab_out[nodev] = nl;
-                changed += (nl != oldv);
-              }
-            }
-          } else {
-            // one vertex per round
-            for (uint32_t j = lo; j < hi; j++) {
-              const uint32_t dv = __shfl_sync(kFull, d, j);
-              const uint32_t *ip =
-                  reinterpret_cast<const uint32_t *>(__shfl_sync(kFull, (unsigned long long)items, j));
-              const uint32_t nodev = __shfl_sync(kFull, node, j);
-              const uint32_t oldv = __shfl_sync(kFull, old, j);
-              uint32_t best;
-              if (dv <= 32) {
-                const bool ok = lane < dv;
-                const uint32_t lab = ok ? __ldg(lab_in + ip[lane]) : kFull;
-                const uint32_t m = __match_any_sync(kFull, lab);
-                const uint32_t cnt = ok ? __popc(m) : 0u;
-                const uint32_t maxc = __reduce_max_sync(kFull, cnt);
-                best = __reduce_min_sync(kFull, (ok && cnt == maxc) ? lab : kFull);
-              } else {
-                const uint32_t cap = next_pow2(2 * dv);
-                for (uint32_t k0 = 0; k0 < dv; k0 += 32) {
-                  const uint32_t k = k0 + lane;
-                  const bool ok = k < dv;
-                  const uint32_t lab = ok ? __ldg(lab_in + ip[k]) : kFull;
-                  const uint32_t m = __match_any_sync(kFull, lab);
-                  if (ok && (__ffs(m) - 1) == int(lane)) table_add(keys, cnts, cap, lab, __popc(m));
-                }
-                __syncwarp();
-                uint64_t bp = 0;
-                for (uint32_t i = lane; i < cap; i += 32) {
-                  const uint32_t kk = keys[i];
-                  if (kk) {
-                    const uint64_t cand = pack_best(cnts[i], kk - 1u);
-                    bp = cand > bp ? cand : bp;
-                    keys[i] = 0u;
-                    cnts[i] = 0u;
-                  }
-                }
-                best = best_label(warp_max_u64(bp));
-                __syncwarp();
-              }
-              if (lane == 0) {
-                const uint32_t nl = dv ? best : oldv;
-                lab_out[nodev] = nl;
-                changed += (nl != oldv);
-              }
-            }
-          }
-        }
-        __syncwarp();
-        done |= batch;
-      }
-    }
-    if (a.seg_cycles) {
-      __syncthreads();
-      if (threadIdx.x == 0) a.seg_cycles[s] = clock64() - t0;
-    }
-  }
-  flush_changed(counter, changed);
-}
-
-__global__ void __launch_bounds__(kLaneWarps * 32) k_lane_batch_packed(IterArgs a) { lane_batch<true>(a); }
-__global__ void __launch_bounds__(kLaneWarps * 32) k_lane_batch_warp(IterArgs a) { lane_batch<false>(a); }
-
-// ---------------------------------------------------------------------------
-// V3: block per vertex.  Threads decode 256-bit segments in parallel; each
-// step every thread contributes at most one item (one residual, or a share of
-// the block-wide flattening of the step's intervals).
-// ---------------------------------------------------------------------------
-struct BlockShared {
-  uint32_t left[kBlockThreads];
-  uint32_t pref[kBlockThreads + 1];
-  uint32_t wsum[kBlockThreads / 32];
-  uint64_t red[kBlockThreads / 32];
-  uint64_t res_start;
-  uint64_t last_end;
-  uint32_t bad;
-  uint32_t items;
-};
-
-// Block-wide exclusive scan of v into sh.pref (pref[kBlockThreads] = total).
-__device__ __forceinline__ uint32_t block_excl_scan(BlockShared &sh, uint32_t v) {
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  uint32_t incl = v;
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, uint32_t lane) {
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t t = __shfl_up_sync(kFull, incl, o);
-    if (lane >= uint32_t(o)) incl += t;
+    const uint32_t t = __shfl_up_sync(kFull, v, o);
+    if (lane >= uint32_t(o)) v += t;
   }
+  return v;
+}
+
+struct BlockSh {
+  uint32_t pref[kThreads + 1];
+  uint32_t left[kThreads];
+  uint32_t wsum[kWarps];
+  uint64_t red[kWarps];
+  uint64_t ibase, rbase, last_end;
+  uint32_t nseg_i, nseg_r, item, items, bad;
+};
+
+// Block-wide exclusive scan of v into sh.pref; returns the total.
+__device__ __forceinline__ uint32_t block_scan(BlockSh &sh, uint32_t v) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t incl = warp_incl_scan(v, lane);
   if (lane == 31) sh.wsum[warp] = incl;
   __syncthreads();
   if (warp == 0) {
-    uint32_t w = lane < kBlockThreads / 32 ? sh.wsum[lane] : 0u;
-    uint32_t wi = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(kFull, wi, o);
-      if (lane >= uint32_t(o)) wi += t;
-    }
-    if (lane < kBlockThreads / 32) sh.wsum[lane] = wi - w;
-    if (lane == kBlockThreads / 32 - 1) sh.pref[kBlockThreads] = wi;
+    const uint32_t w = lane < kWarps ? sh.wsum[lane] : 0u;
+    const uint32_t wi = warp_incl_scan(w, lane);
+    if (lane < kWarps) sh.wsum[lane] = wi - w;
+    if (lane == kWarps - 1) sh.pref[kThreads] = wi;
   }
   __syncthreads();
-  const uint32_t ex = incl - v + sh.wsum[warp];
-  sh.pref[threadIdx.x] = ex;
+  sh.pref[threadIdx.x] = incl - v + sh.wsum[warp];
   __syncthreads();
-  return sh.pref[kBlockThreads];
+  return sh.pref[kThreads];
 }
 
-// Calls consume(ok, id) block-synchronously for every neighbour of position p.
-template <class Consume>
-__device__ __forceinline__ void block_for_each(const IterArgs &a, BlockShared &sh, uint32_t p, uint32_t node,
-                                               uint32_t d, Consume consume) {
+// ------------------------------------------------------------ consumers ---
+// Called warp-synchronously by every lane; ok marks a real label.  Lanes of a
+// warp holding the same label are merged first (match.any), so each distinct
+// label of a step touches the table once.
+struct ExactSink {
+  uint32_t *keys, *cnts, cap;
+  __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
+    const uint32_t m = __match_any_sync(kFull, ok ? lab : kFull);
+    if (ok && (__ffs(m) - 1) == int(threadIdx.x & 31u)) table_add(keys, cnts, cap, lab, __popc(m));
+  }
+};
+
+struct CmsAddSink {
+  uint32_t *cms;
+  const uint32_t *seeds;
+  __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
+    const uint32_t m = __match_any_sync(kFull, ok ? lab : kFull);
+    if (ok && (__ffs(m) - 1) == int(threadIdx.x & 31u)) {
+      const uint32_t c = __popc(m);
+#pragma unroll
+      for (int r = 0; r < kCmsDepth; r++)
+        atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, lab ^ seeds[r]) & (kCmsWidth - 1))], c);
+    }
+  }
+};
+
+struct CmsBestSink {
+  const uint32_t *cms;
+  const uint32_t *seeds;
+  uint64_t *best;
+  __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
+    const uint32_t m = __match_any_sync(kFull, ok ? lab : kFull);
+    if (ok && (__ffs(m) - 1) == int(threadIdx.x & 31u)) {
+      uint32_t est = kFull;
+#pragma unroll
+      for (int r = 0; r < kCmsDepth; r++) {
+        const uint32_t v = cms[r * kCmsWidth + (cm_hash(r, lab ^ seeds[r]) & (kCmsWidth - 1))];
+        est = v < est ? v : est;
+      }
+      const uint64_t cand = pack_best(est, lab);
+      if (cand > *best) *best = cand;
+    }
+  }
+};
+
+// Labels of stage[0..total) in place (ids -> labels), 4 loads in flight per thread.
+__device__ __forceinline__ void block_gather_inplace(uint32_t *stage, uint32_t total,
+                                                     const uint32_t *__restrict__ lab_in) {
+  for (uint32_t k0 = threadIdx.x; k0 < total; k0 += 4 * kThreads) {
+    uint32_t v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t k = k0 + u * kThreads;
+      v[u] = k < total ? __ldg(lab_in + stage[k]) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t k = k0 + u * kThreads;
+      if (k < total) stage[k] = v[u];
+    }
+  }
+}
+
+// Labels of the global ids src[0..total) into stage.
+__device__ __forceinline__ void block_gather_from(uint32_t *stage, const uint32_t *__restrict__ src, uint32_t total,
+                                                  const uint32_t *__restrict__ lab_in) {
+  for (uint32_t k0 = threadIdx.x; k0 < total; k0 += 4 * kThreads) {
+    uint32_t v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t k = k0 + u * kThreads;
+      v[u] = k < total ? __ldg(lab_in + __ldg(src + k)) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t k = k0 + u * kThreads;
+      if (k < total) stage[k] = v[u];
+    }
+  }
+}
+
+template <class Sink>
+__device__ __forceinline__ void block_consume_stage(const uint32_t *stage, uint32_t total, const Sink &sink) {
+  for (uint32_t k0 = 0; k0 < total; k0 += kThreads) {
+    const uint32_t k = k0 + threadIdx.x;
+    const bool ok = k < total;
+    sink(ok, ok ? stage[k] : 0u);
+  }
+}
+
+// Feeds every neighbour label of position p to sink, block-synchronously.
+// Returns true when all labels ended up in stage[0..d) (one chunk, no
+// intervals), so a second pass can read them from there.
+template <class Sink>
+__device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint32_t *stage, uint32_t p,
+                              uint32_t node, uint32_t d, bool from_scratch, const Sink &sink) {
   const DevGraph &g = a.g;
   const uint32_t t = threadIdx.x;
-  uint32_t my_items = 0;
-  if (p >= g.n_c || a.from_scratch) {
-    const uint32_t *ip = (p >= g.n_c) ? g.small_nbr + g.small_off[p - g.n_c] : a.scratch + a.arc_off[p];
-    for (uint32_t k0 = 0; k0 < d; k0 += kBlockThreads) {
-      const uint32_t k = k0 + t;
-      const bool ok = k < d;
-      consume(ok, ok ? ip[k] : 0u);
+  if (p >= g.n_c || from_scratch) {
+    // contiguous ids: the small CSR, or the two-pass scratch
+    const uint32_t *src = (p >= g.n_c) ? g.small_nbr + g.small_off[p - g.n_c] : a.scratch + a.arc_off[p];
+    for (uint32_t c0 = 0; c0 < d; c0 += kStage) {
+      const uint32_t cnt = min(kStage, d - c0);
+      block_gather_from(stage, src + c0, cnt, c.lab_in);
+      __syncthreads();
+      block_consume_stage(stage, cnt, sink);
+      __syncthreads();
     }
-    return;
+    return d <= kStage;
   }
-  const GWords W{g.words};
   const uint64_t end = g.offsets[p + 1];
   bool bad = false;
-  uint64_t q = g.offsets[p];
-  uint32_t nseg = dec_segcnt(W, q, bad);
-  const uint64_t ibase = q;
-  if (q > end || nseg > (end - q) / kSegBits + 1) {  // more segments than bits: malformed
-    bad = true;
-    nseg = 0;
-  }
+  uint32_t my_items = 0;
   if (t == 0) {
-    sh.res_start = q;
-    sh.bad = 0;
+    BitReader r;
+    r.seek(g.words, g.offsets[p]);
+    uint32_t ns = r.segcnt(bad);
+    if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
+      bad = true;
+      ns = 0;
+    }
+    sh.nseg_i = ns;
+    sh.ibase = r.pos;
+    sh.last_end = r.pos;
+    sh.bad = bad ? 1u : 0u;
     sh.items = 0;
   }
   __syncthreads();
-  // interval section
-  for (uint32_t j0 = 0; j0 < nseg; j0 += kBlockThreads) {
+  const uint32_t nseg_i = sh.nseg_i;
+  const uint64_t ibase = sh.ibase;
+  // ---- interval section: pairs decoded one per thread per step, flattened block-wide
+  for (uint32_t j0 = 0; j0 < nseg_i; j0 += kThreads) {
     const uint32_t j = j0 + t;
-    bool has = j < nseg;
-    uint64_t sq = ibase + uint64_t(kSegBits) * j;
-    uint32_t cnt = 0, c = 0, left = 0;
+    bool has = j < nseg_i;
+    BitReader r;
+    uint32_t cnt = 0, cc = 0, left = 0;
+    const uint64_t q = ibase + uint64_t(kSegBits) * j;
     if (has) {
-      if (sq >= end) {
+      if (q >= end) {
         bad = true;
         has = false;
       } else {
-        cnt = dec_gamma(W, sq, bad);
+        r.seek(g.words, q);
+        cnt = r.gamma(bad);
       }
     }
-    while (__syncthreads_or(has && c < cnt)) {
+    while (__syncthreads_or(has && cc < cnt)) {
       uint32_t len = 0;
-      if (has && c < cnt) {
-        const uint32_t l = dec_gamma(W, sq, bad);
-        left = (c == 0) ? zigzag_first(node, l) : left + l + 1u;
-        len = dec_gamma(W, sq, bad) + kMinItv;
-        c++;
-        if (bad || sq > end || uint64_t(left) + len > g.n) {
+      if (has && cc < cnt) {
+        const uint32_t l = r.gamma(bad);
+        left = (cc == 0) ? zigzag_first(node, l) : left + l + 1u;
+        len = r.gamma(bad) + kMinItv;
+        cc++;
+        if (bad || r.pos > end || uint64_t(left) + len > g.n) {
           bad = true;
           len = 0;
-          cnt = c;
+          cnt = cc;
         }
       }
       sh.left[t] = left;
-      const uint32_t total = block_excl_scan(sh, len);
-      if (has && len) left += len;
-      for (uint32_t i0 = 0; i0 < total; i0 += kBlockThreads) {
-        const uint32_t i = i0 + t;
-        const bool ok = i < total;
-        uint32_t id = 0;
-        if (ok) {
-          uint32_t lo = 0, hi = kBlockThreads - 1;
-          while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (sh.pref[mid] <= i) lo = mid;
-            else hi = mid - 1;
+      const uint32_t total = block_scan(sh, len);
+      if (len) left += len;
+      for (uint32_t i0 = 0; i0 < total; i0 += 4 * kThreads) {
+        uint32_t lab[4];
+        bool ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const uint32_t i = i0 + u * kThreads + t;
+          ok[u] = i < total;
+          lab[u] = 0;
+          if (ok[u]) {
+            uint32_t lo = 0, hi = kThreads - 1;
+            while (lo < hi) {
+              const uint32_t mid = (lo + hi + 1) >> 1;
+              if (sh.pref[mid] <= i) lo = mid;
+              else hi = mid - 1;
+            }
+            lab[u] = __ldg(c.lab_in + sh.left[lo] + (i - sh.pref[lo]));
+            my_items++;
           }
-          id = sh.left[lo] + (i - sh.pref[lo]);
-          my_items++;
         }
-        consume(ok, id);
+#pragma unroll
+        for (int u = 0; u < 4; u++) sink(ok[u], lab[u]);
       }
       __syncthreads();
     }
-    if (has && j == nseg - 1) sh.res_start = sq;
+    if (has && j == nseg_i - 1) sh.last_end = r.pos;
   }
   __syncthreads();
-  // residual section
-  q = sh.res_start;
-  uint32_t nres = dec_segcnt(W, q, bad);
-  const uint64_t rbase = q;
-  if (q > end || nres > (end - q) / kSegBits + 1) {
-    bad = true;
-    nres = 0;
+  // ---- residual section: rounds of up to kResSegChunk segments staged in shared memory
+  if (t == 0) {
+    BitReader r;
+    r.seek(g.words, sh.last_end);
+    uint32_t ns = r.segcnt(bad);
+    if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
+      bad = true;
+      ns = 0;
+    }
+    sh.nseg_r = ns;
+    sh.rbase = r.pos;
+    sh.last_end = r.pos;
   }
-  if (t == 0) sh.last_end = q;
   __syncthreads();
-  for (uint32_t j0 = 0; j0 < nres; j0 += kBlockThreads) {
+  const uint32_t nseg_r = sh.nseg_r;
+  const uint64_t rbase = sh.rbase;
+  for (uint32_t j0 = 0; j0 < nseg_r; j0 += kResSegChunk) {
     const uint32_t j = j0 + t;
-    bool has = j < nres;
-    uint64_t sq = rbase + uint64_t(kSegBits) * j;
-    uint32_t cnt = 0, c = 0, v = 0;
+    bool has = t < kResSegChunk && j < nseg_r;
+    BitReader r;
+    uint32_t cnt = 0;
+    const uint64_t q = rbase + uint64_t(kSegBits) * j;
     if (has) {
-      if (sq >= end) {
+      if (q >= end) {
         bad = true;
         has = false;
       } else {
-        cnt = dec_gamma(W, sq, bad);
-      }
-    }
-    while (__syncthreads_or(has && c < cnt)) {
-      bool ok = has && c < cnt;
-      if (ok) {
-        const uint32_t x = dec_zeta3(W, sq, bad);
-        v = (c == 0) ? zigzag_first(node, x) : v + x + 1u;
-        c++;
-        if (bad || sq > end || uint64_t(v) >= g.n) {
+        r.seek(g.words, q);
+        cnt = r.gamma(bad);
+        if (bad || cnt > kStage) {
           bad = true;
-          ok = false;
-          cnt = c;
-        } else {
-          my_items++;
+          cnt = 0;
         }
       }
-      consume(ok, v);
     }
-    if (has && j == nres - 1) sh.last_end = sq;
+    const uint32_t total = block_scan(sh, cnt);
+    if (total > kStage) {  // more items than a round of well-formed segments can hold
+      if (t == 0) sh.bad = 1;
+      __syncthreads();
+      break;
+    }
+    if (has) {
+      uint32_t o = sh.pref[t], v = 0;
+      for (uint32_t cc = 0; cc < cnt; cc++) {
+        const uint32_t x = r.zeta3(bad);
+        v = (cc == 0) ? zigzag_first(node, x) : v + x + 1u;
+        if (bad || r.pos > end || uint64_t(v) >= g.n) {
+          bad = true;
+          v = node;  // keeps the staged id in range; the error word reports the stream
+        }
+        stage[o++] = v;
+      }
+      my_items += cnt;
+      if (j == nseg_r - 1) sh.last_end = r.pos;
+    }
+    __syncthreads();
+    block_gather_inplace(stage, total, c.lab_in);
+    __syncthreads();
+    block_consume_stage(stage, total, sink);
+    __syncthreads();
   }
   if (my_items) atomicAdd(&sh.items, my_items);
   if (bad) sh.bad = 1;
   __syncthreads();
   if (t == 0 && (sh.bad || sh.last_end != end || sh.items != d)) set_error(a.err, kErrBadStream);
-  __syncthreads();
+  return nseg_i == 0 && nseg_r <= kResSegChunk;
 }
 
-__global__ void __launch_bounds__(kBlockThreads) k_block(IterArgs a) {
-  extern __shared__ uint32_t smem[];
-  __shared__ BlockShared sh;
-  uint32_t *skeys = smem, *scnts = smem + kBlockSlots;
-  uint32_t *cms = smem;  // depth x width counters share the table memory
+// One heavy vertex by the whole block.
+__device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint32_t *stage, uint32_t *tab,
+                             uint32_t seg, uint32_t p, bool from_scratch, unsigned long long &changed) {
   const DevGraph &g = a.g;
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
-  const uint32_t *lab_in;
-  uint32_t *lab_out;
-  unsigned long long *counter;
-  resolve_iter(a, lab_in, lab_out, counter);
-  unsigned long long changed = 0;
-  for (uint32_t i = t; i < 2 * kBlockSlots; i += kBlockThreads) smem[i] = 0u;  // tables start empty
-  __syncthreads();
-
-  for (uint32_t li = blockIdx.x; li < a.n_list; li += gridDim.x) {
-    const uint32_t s = a.seg_list[li];
-    const Seg seg = a.segs[s];
-    const long long t0 = clock64();
-    for (uint32_t p = seg.begin; p < seg.end; p++) {
-      const uint32_t node = g.vertices[p];
-      const uint32_t d = g.deg[p];
-      const uint32_t old = __ldg(lab_in + node);
-      if (d == 0) continue;
-      const bool use_cms = a.cms_thr != 0 && d >= a.cms_thr;
-      uint64_t bp = 0;
-      if (use_cms) {
-        block_for_each(a, sh, p, node, d, [&](bool ok, uint32_t id) {
-          const uint32_t lab = ok ? __ldg(lab_in + id) : kFull;
-          const uint32_t m = __match_any_sync(kFull, lab);
-          if (ok && (__ffs(m) - 1) == int(lane)) {
-            const uint32_t c = __popc(m);
-#pragma unroll
-            for (int r = 0; r < kCmsDepth; r++)
-              atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, lab ^ a.seeds[r]) & (kCmsWidth - 1))], c);
-          }
-        });
-        __syncthreads();
-        block_for_each(a, sh, p, node, d, [&](bool ok, uint32_t id) {
-          if (ok) {
-            const uint32_t lab = __ldg(lab_in + id);
-            uint32_t est = kFull;
-#pragma unroll
-            for (int r = 0; r < kCmsDepth; r++) {
-              const uint32_t cv = cms[r * kCmsWidth + (cm_hash(r, lab ^ a.seeds[r]) & (kCmsWidth - 1))];
-              est = cv < est ? cv : est;
-            }
-            const uint64_t cand = pack_best(est, lab);
-            bp = cand > bp ? cand : bp;
-          }
-        });
-        __syncthreads();
-        for (uint32_t i = t; i < kCmsDepth * kCmsWidth; i += kBlockThreads) cms[i] = 0u;
-      } else {
-        uint32_t *keys, *cnts;
-        const uint32_t cap = next_pow2(2 * d);
-        if (d <= kBlockMaxSmemDeg) {
-          keys = skeys;
-          cnts = scnts;
-        } else {
-          if (a.gtab_slots == 0 || cap > a.gtab_slots) {
-            set_error(a.err, kErrCapacity);
-            continue;
-          }
-          keys = a.gtab + uint64_t(blockIdx.x) * 2 * a.gtab_slots;
-          cnts = keys + a.gtab_slots;
-        }
-        block_for_each(a, sh, p, node, d, [&](bool ok, uint32_t id) {
-          const uint32_t lab = ok ? __ldg(lab_in + id) : kFull;
-          const uint32_t m = __match_any_sync(kFull, lab);
-          if (ok && (__ffs(m) - 1) == int(lane)) table_add(keys, cnts, cap, lab, __popc(m));
-        });
-        __syncthreads();
-        for (uint32_t i = t; i < cap; i += kBlockThreads) {
-          const uint32_t kk = keys[i];
-          if (kk) {
-            const uint64_t cand = pack_best(cnts[i], kk - 1u);
-            bp = cand > bp ? cand : bp;
-            keys[i] = 0u;
-            cnts[i] = 0u;
-          }
-        }
+  const uint32_t node = g.vertices[p];
+  const uint32_t d = g.deg[p];
+  const uint32_t old = __ldg(c.lab_in + node);
+  if (d == 0) return;
+  uint64_t best = 0;
+  if (a.cms_thr != 0 && d >= a.cms_thr) {
+    uint32_t *cms = tab;  // zero on entry
+    const bool staged = heavy_produce(a, c, sh, stage, p, node, d, from_scratch, CmsAddSink{cms, a.seeds});
+    __syncthreads();
+    CmsBestSink s2{cms, a.seeds, &best};
+    if (staged) block_consume_stage(stage, d, s2);
+    else heavy_produce(a, c, sh, stage, p, node, d, from_scratch, s2);
+    __syncthreads();
+    for (uint32_t i = t; i < kCmsDepth * kCmsWidth; i += kThreads) cms[i] = 0u;
+  } else {
+    uint32_t *keys, *cnts;
+    const uint32_t cap = next_pow2(2 * d);
+    if (d <= kBlockMaxSmemDeg) {
+      keys = tab;
+      cnts = tab + kTableSlots;
+    } else {
+      if (a.gtab_slots == 0 || cap > a.gtab_slots) {
+        if (t == 0) set_error(a.err, kErrCapacity);
+        return;
       }
-      bp = warp_max_u64(bp);
-      if (lane == 0) sh.red[warp] = bp;
-      __syncthreads();
-      if (t == 0) {
-        uint64_t b = 0;
-        for (int w = 0; w < kBlockThreads / 32; w++) b = sh.red[w] > b ? sh.red[w] : b;
-        const uint32_t nl = b ? best_label(b) : old;
-        lab_out[node] = nl;
-        changed += (nl != old);
-      }
-      __syncthreads();
+      keys = a.gtab + uint64_t(blockIdx.x) * 2 * a.gtab_slots;
+      cnts = keys + a.gtab_slots;
     }
-    if (a.seg_cycles && t == 0) a.seg_cycles[s] = clock64() - t0;
+    heavy_produce(a, c, sh, stage, p, node, d, from_scratch, ExactSink{keys, cnts, cap});
+    __syncthreads();
+    for (uint32_t i = t; i < cap; i += kThreads) {
+      const uint32_t kk = keys[i];
+      if (kk) {
+        const uint64_t cand = pack_best(cnts[i], kk - 1u);
+        best = cand > best ? cand : best;
+        keys[i] = 0u;
+        cnts[i] = 0u;
+      }
+    }
   }
-  flush_changed(counter, changed);
+  best = warp_max_u64(best);
+  if (lane == 0) sh.red[warp] = best;
+  __syncthreads();
+  if (t == 0) {
+    uint64_t b = 0;
+    for (int w = 0; w < kWarps; w++) b = sh.red[w] > b ? sh.red[w] : b;
+    const uint32_t nl = b ? best_label(b) : old;
+    c.lab_out[node] = nl;
+    changed += (nl != old);
+    if (a.seg_changed && nl != old) atomicAdd(a.seg_changed + seg, 1u);
+  }
+  __syncthreads();
 }
 
-// ---------------------------------------------------------------------------
-// Decode positions into a CSR scratch (two-pass variant, parity hook).
-// ---------------------------------------------------------------------------
+// Up to 32 consecutive positions [p0, p1) by one warp.
+__device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, uint32_t *keys, uint32_t *cnts,
+                            uint32_t seg, uint32_t p0, uint32_t p1, int variant, unsigned long long &changed) {
+  const DevGraph &g = a.g;
+  const uint32_t lane = threadIdx.x & 31u;
+  constexpr uint32_t cap_stage = kStage / kWarps;
+  const uint32_t p = p0 + lane;
+  const bool valid = p < p1;
+  const uint32_t node = valid ? g.vertices[p] : 0u;
+  uint32_t d = valid ? g.deg[p] : 0u;
+  const uint32_t old = valid ? __ldg(c.lab_in + node) : 0u;
+  const bool cgr = p0 < g.n_c;  // chunks never straddle the compressed / small boundary
+  const bool decode = cgr && variant != kVarTwoPass;
+  if (d > cap_stage || (variant == kVarPacked && d > kV2MaxDeg) || d > kV1MaxDeg) {
+    set_error(a.err, kErrCapacity);
+    d = 0;
+  }
+  // contiguous id source of the chunk when it is not decoded here
+  const uint32_t *src = nullptr;
+  if (!decode) src = cgr ? a.scratch + a.arc_off[p0] : g.small_nbr + g.small_off[p0 - g.n_c];
+  uint32_t src_skip = 0;  // ids consumed by earlier batches of this chunk
+  uint32_t done = ~__ballot_sync(kFull, valid);
+  uint32_t my_changed = 0;
+  while (done != kFull) {
+    const bool pending = !((done >> lane) & 1u);
+    const uint32_t sd = pending ? d : 0u;
+    const uint32_t incl = warp_incl_scan(sd, lane);
+    const bool in_batch = pending && incl <= cap_stage;
+    const uint32_t batch = __ballot_sync(kFull, in_batch);
+    const uint32_t lo = __ffs(batch) - 1, hi = 32 - __clz(batch);
+    const uint32_t total = __shfl_sync(kFull, incl, hi - 1);
+    const uint32_t base = incl - sd;
+    // 1. ids (decoded lane-per-vertex)
+    if (decode && in_batch && d) {
+      uint32_t k = 0;
+      const int64_t r = walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], node, g.n, [&](uint32_t id) {
+        if (k < d) stage[base + k] = id;
+        k++;
+      });
+      if (r != int64_t(d)) {
+        set_error(a.err, kErrBadStream);
+        for (uint32_t q = (r > 0 ? uint32_t(r) : 0u); q < d; q++) stage[base + q] = node;
+      }
+    }
+    __syncwarp();
+    // 2. labels: every load of the batch in flight together
+    for (uint32_t k0 = lane; k0 < total; k0 += 128) {
+      uint32_t v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint32_t k = k0 + 32 * u;
+        v[u] = k < total ? __ldg(c.lab_in + (decode ? stage[k] : __ldg(src + src_skip + k))) : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint32_t k = k0 + 32 * u;
+        if (k < total) stage[k] = v[u];
+      }
+    }
+    __syncwarp();
+    // 3. count
+    const uint32_t dmax = __reduce_max_sync(kFull, in_batch ? d : 0u);
+    if (dmax <= 32 && (variant == kVarPacked || dmax <= 1)) {
+      // several vertices per round: G lanes per vertex
+      const uint32_t G = next_pow2(dmax);
+      const uint32_t per = 32 / G;
+      const uint32_t gl = lane / G, k = lane % G;
+      const uint32_t gm = (G == 32) ? kFull : (((1u << G) - 1u) << (gl * G));
+      for (uint32_t v0 = lo; v0 < hi; v0 += per) {
+        const uint32_t vi = v0 + gl;
+        const bool vin = vi < hi;
+        const uint32_t srcl = vin ? vi : lo;
+        const uint32_t dv = __shfl_sync(kFull, d, srcl);
+        const uint32_t bv = __shfl_sync(kFull, base, srcl);
+        const uint32_t nodev = __shfl_sync(kFull, node, srcl);
+        const uint32_t oldv = __shfl_sync(kFull, old, srcl);
+        const bool ok = vin && k < dv;
+        const uint32_t lab = ok ? stage[bv + k] : kFull;
+        const uint32_t m = __match_any_sync(kFull, (uint64_t(gl) << 32) | lab);
+        const uint32_t cnt = ok ? __popc(m) : 0u;
+        const uint32_t maxc = __reduce_max_sync(gm, cnt);
+        const uint32_t bestl = __reduce_min_sync(gm, (ok && cnt == maxc) ? lab : kFull);
+        if (vin && k == 0) {
+          const uint32_t nl = dv ? bestl : oldv;
+          c.lab_out[nodev] = nl;
+          my_changed += (nl != oldv);
+        }
+      }
+    } else {
+      // one vertex per round
+      for (uint32_t j = lo; j < hi; j++) {
+        const uint32_t dv = __shfl_sync(kFull, d, j);
+        const uint32_t bv = __shfl_sync(kFull, base, j);
+        const uint32_t nodev = __shfl_sync(kFull, node, j);
+        const uint32_t oldv = __shfl_sync(kFull, old, j);
+        uint32_t bestl;
+        if (dv <= 32) {
+          const bool ok = lane < dv;
+          const uint32_t lab = ok ? stage[bv + lane] : kFull;
+          const uint32_t m = __match_any_sync(kFull, lab);
+          const uint32_t cnt = ok ? __popc(m) : 0u;
+          const uint32_t maxc = __reduce_max_sync(kFull, cnt);
+          bestl = __reduce_min_sync(kFull, (ok && cnt == maxc) ? lab : kFull);
+        } else {
+          const uint32_t cap = next_pow2(2 * dv);
+          for (uint32_t k0 = 0; k0 < dv; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            const bool ok = k < dv;
+            const uint32_t lab = ok ? stage[bv + k] : kFull;
+            const uint32_t m = __match_any_sync(kFull, lab);
+            if (ok && (__ffs(m) - 1) == int(lane)) table_add(keys, cnts, cap, lab, __popc(m));
+          }
+          __syncwarp();
+          uint64_t bp = 0;
+          for (uint32_t i = lane; i < cap; i += 32) {
+            const uint32_t kk = keys[i];
+            if (kk) {
+              const uint64_t cand = pack_best(cnts[i], kk - 1u);
+              bp = cand > bp ? cand : bp;
+              keys[i] = 0u;
+              cnts[i] = 0u;
+            }
+          }
+          bestl = best_label(warp_max_u64(bp));
+          __syncwarp();
+        }
+        if (lane == 0) {
+          const uint32_t nl = dv ? bestl : oldv;
+          c.lab_out[nodev] = nl;
+          my_changed += (nl != oldv);
+        }
+      }
+    }
+    __syncwarp();
+    src_skip += total;
+    done |= batch;
+  }
+  changed += my_changed;
+  if (a.seg_changed) {
+    const uint32_t s = __reduce_add_sync(kFull, my_changed);
+    if (lane == 0 && s) atomicAdd(a.seg_changed + seg, s);
+  }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads, 3) k_iterate(IterArgs a) {
+  extern __shared__ uint32_t smem[];
+  __shared__ BlockSh sh;
+  uint32_t *stage = smem;         // kStage words
+  uint32_t *tab = smem + kStage;  // kTableSlots keys + kTableSlots counts (or the sketch)
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  for (uint32_t i = t; i < 2 * kTableSlots; i += kThreads) tab[i] = 0u;
+  __syncthreads();
+  const Ctx c = resolve(a);
+  unsigned long long changed = 0;
+  uint32_t *qctr = a.work + 2 * (a.it_dev ? c.it : 0u);
+
+  // heavy items: one segment per block (largest first)
+  for (;;) {
+    if (t == 0) sh.item = atomicAdd(qctr, 1u);
+    __syncthreads();
+    const uint32_t i = sh.item;
+    __syncthreads();
+    if (i >= a.n_heavy) break;
+    const uint32_t s = a.heavy[i];
+    const bool from_scratch = a.seg_var[s] == kVarTwoPass;
+    const Seg sg = a.segs[s];
+    const long long t0 = clock64();
+    for (uint32_t p = sg.begin; p < sg.end; p++) heavy_vertex(a, c, sh, stage, tab, s, p, from_scratch, changed);
+    if (a.seg_cycles && t == 0)
+      atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s),
+                (unsigned long long)((clock64() - t0) * kWarps));
+  }
+
+  // light chunks: one warp per chunk of up to 32 positions
+  uint32_t *wkeys = tab + warp * kWarpSlots;
+  uint32_t *wcnts = tab + kTableSlots + warp * kWarpSlots;
+  uint32_t *wstage = stage + warp * (kStage / kWarps);
+  for (;;) {
+    uint32_t i = 0;
+    if (lane == 0) i = atomicAdd(qctr + 1, 1u);
+    i = __shfl_sync(kFull, i, 0);
+    if (i >= a.n_light) break;
+    const uint32_t item = a.light[i];
+    const uint32_t s = item >> 3;
+    const Seg sg = a.segs[s];
+    const uint32_t p0 = sg.begin + (item & 7u) * 32u;
+    const long long t0 = clock64();
+    light_chunk(a, c, wstage, wkeys, wcnts, s, p0, min(sg.end, p0 + 32u), a.seg_var[s], changed);
+    if (a.seg_cycles && lane == 0)
+      atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s), (unsigned long long)(clock64() - t0));
+  }
+  flush_changed(c.changed, changed);
+}
+
+// Two-pass variant, pass 1: decode the two-pass segments' compressed positions
+// into the scratch CSR (block per segment, thread per position).
+__global__ void __launch_bounds__(kThreads) k_decode_two_pass(IterArgs a) {
+  const DevGraph &g = a.g;
+  for (uint32_t i = blockIdx.x; i < a.n_two_pass; i += gridDim.x) {
+    const uint32_t s = a.two_pass[i];
+    const Seg sg = a.segs[s];
+    if (sg.begin >= g.n_c) continue;
+    const long long t0 = clock64();
+    for (uint32_t p = sg.begin + threadIdx.x; p < sg.end; p += kThreads) {
+      uint32_t *dst = a.scratch + a.arc_off[p];
+      const uint32_t d = g.deg[p];
+      uint32_t k = 0;
+      const int64_t r = walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], g.vertices[p], g.n,
+                                        [&](uint32_t id) {
+                                          if (k < d) dst[k] = id;
+                                          k++;
+                                        });
+      if (r != int64_t(d)) {
+        set_error(a.err, kErrBadStream);
+        for (uint32_t q = (r > 0 ? uint32_t(r) : 0u); q < d; q++) dst[q] = g.vertices[p];
+      }
+    }
+    if (a.seg_cycles && threadIdx.x == 0)
+      atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s),
+                (unsigned long long)((clock64() - t0) * kWarps));
+  }
+}
+
+// Decode positions into a CSR scratch (parity hook).
 __global__ void k_decode_positions(DecodeArgs a) {
   const DevGraph &g = a.g;
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < a.n_pos;
@@ -486,40 +649,22 @@ __global__ void k_decode_positions(DecodeArgs a) {
   }
 }
 
-// Two-pass variant, pass 1: block per segment, thread per position.
-__global__ void k_decode_segments(IterArgs a) {
-  const DevGraph &g = a.g;
-  for (uint32_t li = blockIdx.x; li < a.n_list; li += gridDim.x) {
-    const Seg seg = a.segs[a.seg_list[li]];
-    for (uint32_t p = seg.begin + threadIdx.x; p < seg.end; p += blockDim.x) {
-      if (p >= g.n_c) continue;
-      uint32_t *dst = const_cast<uint32_t *>(a.scratch) + a.arc_off[p];
-      const uint32_t d = g.deg[p];
-      uint32_t k = 0;
-      const int64_t r = walk_vertex(GWords{g.words}, g.offsets[p], g.offsets[p + 1], g.vertices[p], g.n,
-                                    [&](uint32_t id) {
-                                      if (k < d) dst[k] = id;
-                                      k++;
-                                    });
-      if (r != int64_t(d)) {
-        set_error(a.err, kErrBadStream);
-        for (uint32_t q = (r > 0 ? uint32_t(r) : 0u); q < d; q++) dst[q] = g.vertices[p];
-      }
-    }
-  }
-}
-
-__global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *err) {
+__global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *itv_out, uint32_t *err) {
   for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < g.n;
        p += uint64_t(gridDim.x) * blockDim.x) {
-    uint32_t d = 0;
+    uint32_t d = 0, itv = 0;
     if (g.vertices[p] >= g.n) {
       set_error(err, kErrBadStream);
     } else if (p < g.n_c) {
-      const int64_t c = walk_vertex(GWords{g.words}, g.offsets[p], g.offsets[p + 1], g.vertices[p], g.n,
-                                    [](uint32_t) {});
-      if (c < 0 || c > int64_t(0xFFFFFFFFll)) set_error(err, kErrBadStream);
-      else d = uint32_t(c);
+      int64_t iv = 0;
+      const int64_t c = walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], g.vertices[p], g.n,
+                                        [](uint32_t) {}, &iv);
+      if (c < 0 || c > int64_t(0xFFFFFFFFll)) {
+        set_error(err, kErrBadStream);
+      } else {
+        d = uint32_t(c);
+        itv = uint32_t(iv);
+      }
     } else {
       const uint32_t b = g.small_off[p - g.n_c], e = g.small_off[p - g.n_c + 1];
       if (e < b) {
@@ -535,6 +680,7 @@ __global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *err) {
       }
     }
     deg_out[p] = d;
+    if (itv_out) itv_out[p] = itv;
   }
 }
 

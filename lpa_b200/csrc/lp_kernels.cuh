@@ -11,19 +11,24 @@ namespace lpa_dev {
 enum Variant : int {
   kVarWarp = 0,     // V1: lane-per-vertex decode, warp-per-vertex counting (deg <= kV1MaxDeg)
   kVarPacked = 1,   // V2: lane-per-vertex decode, several vertices per warp counting (deg <= 32)
-  kVarBlock = 2,    // V3: block-per-vertex, segment-parallel decode, block table / sketch
-  kVarTwoPass = 3,  // V4: decode to a CSR scratch, then count from it
+  kVarBlock = 2,    // V3: block per vertex, segment-parallel decode, block table / sketch
+  kVarTwoPass = 3,  // V4: a decode pass writes a CSR scratch; counting reads it
   kNumVariants = 4
 };
 
-constexpr int kLaneWarps = 8;        // warps per block in the lane-batch kernel
-constexpr uint32_t kStage = 1024;    // staged neighbour ids per warp
-constexpr uint32_t kV1Slots = 512;   // exact-count table slots per warp (V1)
-constexpr uint32_t kV1MaxDeg = kV1Slots / 2;
+constexpr int kThreads = 256;             // threads per block of the iteration kernel
+constexpr int kWarps = kThreads / 32;
+constexpr uint32_t kStage = 8192;         // staged ids/labels per block
+constexpr uint32_t kTableSlots = 4096;    // exact-count slots per block
+constexpr uint32_t kWarpSlots = kTableSlots / kWarps;  // per warp in warp-counting mode
+constexpr uint32_t kV1MaxDeg = kWarpSlots / 2;         // 256
 constexpr uint32_t kV2MaxDeg = 32;
-constexpr int kBlockThreads = 256;   // V3 block size
-constexpr uint32_t kBlockSlots = 8192;  // V3 shared exact-count table slots
-constexpr uint32_t kBlockMaxSmemDeg = kBlockSlots / 2;
+constexpr uint32_t kBlockMaxSmemDeg = kTableSlots / 2; // exact degrees counted in shared memory
+constexpr uint32_t kTileMax = kThreads;   // positions per light tile (one per thread)
+constexpr uint32_t kResSegChunk = 128;    // residual segments staged per round (<= 64 items each)
+
+// dynamic shared memory of the iteration kernel
+constexpr size_t kSmemBytes = size_t(kStage) * 4 + size_t(kTableSlots) * 8;
 
 struct Seg {
   uint32_t begin, end;  // positions [begin, end)
@@ -35,35 +40,32 @@ struct IterArgs {
   uint32_t parity0;             // iteration 0 of this launch reads labs0 when 0, labs1 when 1
   const uint32_t *it_dev;       // device iteration counter (CUDA-graph loop), nullptr: 0
   unsigned long long *changed;  // changed counters, indexed by the iteration counter
+  uint32_t *work;               // work-queue counters, indexed by the iteration counter
   uint32_t *err;
   const Seg *segs;              // all segments
-  const uint32_t *seg_list;     // segments handled by this launch
-  uint32_t n_list;
+  const uint8_t *seg_var;       // variant per segment
+  const uint32_t *heavy;        // block work items: segment ids, largest first
+  uint32_t n_heavy;
+  const uint32_t *light;        // warp work items: (segment << 3) | 32-position chunk
+  uint32_t n_light;
+  const uint32_t *two_pass;     // segments decoded by the two-pass pre-pass
+  uint32_t n_two_pass;
   long long *seg_cycles;        // per-segment device cycles (nullptr: off)
+  uint32_t *seg_changed;        // per-segment changed counts (nullptr: off)
   uint32_t cms_thr;             // 0: no sketch
   uint32_t seeds[kCmsDepth];
   // two-pass scratch: ids of compressed position p at scratch[arc_off[p]..)
-  const uint32_t *scratch;
+  uint32_t *scratch;
   const uint64_t *arc_off;
-  int from_scratch;             // count from the scratch instead of decoding
-  // global exact-count tables for V3 vertices above kBlockMaxSmemDeg
+  // global exact-count tables for exact vertices above kBlockMaxSmemDeg
   uint32_t *gtab;
   uint32_t gtab_slots;          // slots per block (power of two), 0: none
 };
 
-// Resolves this launch's input/output buffers and changed counter.
-__device__ __forceinline__ void resolve_iter(const IterArgs &a, const uint32_t *&lab_in, uint32_t *&lab_out,
-                                             unsigned long long *&changed) {
-  const uint32_t it = a.it_dev ? *a.it_dev : 0u;
-  const uint32_t par = (a.parity0 + it) & 1u;
-  lab_in = par ? a.labs1 : a.labs0;
-  lab_out = par ? a.labs0 : a.labs1;
-  changed = a.changed + (a.it_dev ? it : 0u);
-}
+__device__ __forceinline__ uint32_t iter_index(const IterArgs &a) { return a.it_dev ? *a.it_dev : 0u; }
 
-__global__ void k_lane_batch_packed(IterArgs a);
-__global__ void k_lane_batch_warp(IterArgs a);
-__global__ void k_block(IterArgs a);
+__global__ void k_iterate(IterArgs a);
+__global__ void k_decode_two_pass(IterArgs a);
 
 struct DecodeArgs {
   DevGraph g;
@@ -74,9 +76,8 @@ struct DecodeArgs {
   uint32_t *err;
 };
 __global__ void k_decode_positions(DecodeArgs a);
-__global__ void k_decode_segments(IterArgs a);
 
-__global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *err);
+__global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *itv_out, uint32_t *err);
 __global__ void k_init_labels(uint32_t *a, uint32_t *b, uint64_t n);
 
 }  // namespace lpa_dev

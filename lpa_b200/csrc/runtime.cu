@@ -19,8 +19,9 @@ namespace {
 
 constexpr int kMaxRunSlots = 1 << 16;
 
-// Segment cutting limits per bucket: positions and arcs.
-constexpr uint32_t kSegPositions[kNumBuckets] = {1024, 256, 64, 1};
+// Segment cutting limits per bucket: positions (light segments hold at most
+// 8 warp chunks of 32) and arcs.
+constexpr uint32_t kSegPositions[kNumBuckets] = {256, 256, 64, 1};
 constexpr uint64_t kSegArcs = 16384;
 
 struct Fail {
@@ -178,53 +179,47 @@ static void build_segments(lpa_handle *h) {
 }
 
 static void upload_lists(lpa_handle *h) {
-  std::vector<uint32_t> lists[kNumLists];
+  // heavy items: segments counted by a whole block (largest first); light
+  // items: 32-position chunks of the others; two-pass segments of the
+  // compressed region are decoded by the pre-pass.
+  std::vector<uint32_t> heavy, light, two;
   for (size_t s = 0; s < h->segs.size(); s++) {
     const int v = h->variant[s];
     const SegInfo &si = h->segs[s];
-    switch (v) {
-      case LPA_VARIANT_WARP:
-        lists[kListWarp].push_back(uint32_t(s));
-        break;
-      case LPA_VARIANT_PACKED:
-        lists[kListPacked].push_back(uint32_t(s));
-        break;
-      case LPA_VARIANT_BLOCK:
-        lists[kListBlock].push_back(uint32_t(s));
-        break;
-      default:
-        if (variant_capable(LPA_VARIANT_WARP, si, h->opts.cms_threshold))
-          lists[kListTwoLight].push_back(uint32_t(s));
-        else
-          lists[kListTwoHeavy].push_back(uint32_t(s));
+    const bool block = v == LPA_VARIANT_BLOCK ||
+                       (v == LPA_VARIANT_TWO_PASS && !variant_capable(LPA_VARIANT_WARP, si, h->opts.cms_threshold));
+    if (block) {
+      heavy.push_back(uint32_t(s));
+    } else {
+      const uint32_t chunks = (si.end - si.begin + 31) / 32;
+      for (uint32_t c = 0; c < chunks; c++) light.push_back((uint32_t(s) << 3) | c);
     }
+    if (v == LPA_VARIANT_TWO_PASS && si.region == 0) two.push_back(uint32_t(s));
   }
+  std::stable_sort(heavy.begin(), heavy.end(),
+                   [&](uint32_t a, uint32_t b) { return h->segs[a].arcs > h->segs[b].arcs; });
+  h->n_heavy = uint32_t(heavy.size());
+  h->n_light = uint32_t(light.size());
+  h->n_two_pass = uint32_t(two.size());
   std::vector<uint32_t> all;
-  for (int l = 0; l < kNumLists; l++) {
-    h->list_off[l] = uint32_t(all.size());
-    all.insert(all.end(), lists[l].begin(), lists[l].end());
+  all.reserve(heavy.size() + light.size() + two.size());
+  all.insert(all.end(), heavy.begin(), heavy.end());
+  all.insert(all.end(), light.begin(), light.end());
+  all.insert(all.end(), two.begin(), two.end());
+  if (all.size() > h->lists_cap) {
+    if (h->d_lists) {
+      auto it = std::find(h->allocations.begin(), h->allocations.end(), (void *)h->d_lists);
+      if (it != h->allocations.end()) h->allocations.erase(it);
+      cudaFree(h->d_lists);
+    }
+    h->lists_cap = all.size() + all.size() / 4 + 16;
+    h->d_lists = dalloc<uint32_t>(h, h->lists_cap, "work lists");
   }
-  h->list_off[kNumLists] = uint32_t(all.size());
-  h->v4_all_off = h->list_off[kListTwoLight];
-  h->v4_all_n = h->list_off[kListTwoHeavy + 1] - h->list_off[kListTwoLight];
-  if (!h->d_lists) h->d_lists = dalloc<uint32_t>(h, h->segs.size() + 1, "segment lists");
-  h2d(h, h->d_lists, all.data(), all.size(), "upload segment lists");
-  check(h, cudaStreamSynchronize(h->stream), "upload segment lists");
+  h2d(h, h->d_lists, all.data(), all.size(), "upload work lists");
+  h2d(h, h->d_seg_var, h->variant.data(), h->variant.size(), "upload variants");
+  check(h, cudaStreamSynchronize(h->stream), "upload work lists");
   h->plan_version++;
-
-  auto grid_for = [&](uint32_t nlist, int occ) {
-    return int(std::max<uint64_t>(1, std::min<uint64_t>(nlist, uint64_t(h->num_sms) * uint64_t(occ))));
-  };
-  h->grid[kListWarp] = grid_for(h->list_off[kListWarp + 1] - h->list_off[kListWarp], h->occ_warp);
-  h->grid[kListPacked] = grid_for(h->list_off[kListPacked + 1] - h->list_off[kListPacked], h->occ_packed);
-  h->grid[kListBlock] = grid_for(h->list_off[kListBlock + 1] - h->list_off[kListBlock], h->occ_block);
-  h->grid[kListTwoLight] = grid_for(h->list_off[kListTwoLight + 1] - h->list_off[kListTwoLight], h->occ_warp);
-  h->grid[kListTwoHeavy] = grid_for(h->list_off[kListTwoHeavy + 1] - h->list_off[kListTwoHeavy], h->occ_block);
-  h->grid_decode = grid_for(h->v4_all_n, 8);
-  if (h->gtab_slots) {
-    h->grid[kListBlock] = std::min(h->grid[kListBlock], h->gtab_blocks);
-    h->grid[kListTwoHeavy] = std::min(h->grid[kListTwoHeavy], h->gtab_blocks);
-  }
+  h->grid_decode = int(std::max<uint64_t>(1, std::min<uint64_t>(h->n_two_pass, uint64_t(h->num_sms) * 4)));
 }
 
 static void ensure_two_pass_scratch(lpa_handle *h) {
@@ -253,10 +248,12 @@ static void apply_dispatch(lpa_handle *h, int dispatch, int force) {
 static void build_plan(lpa_handle *h) {
   // degrees, decoded once on the device (validates the stream as well)
   h->d_deg = dalloc<uint32_t>(h, h->n, "degrees");
+  uint32_t *d_itv = nullptr;
+  check(h, cudaMalloc(&d_itv, std::max<uint64_t>(1, h->n) * sizeof(uint32_t)), "interval counts");
   {
-    const int threads = 256;
-    const int blocks = int(std::min<uint64_t>((h->n + threads - 1) / threads, uint64_t(h->num_sms) * 16));
-    k_degree_count<<<std::max(blocks, 1), threads, 0, h->stream>>>(dev_graph(h), h->d_deg, h->d_err);
+    const int threads = 128;
+    const int blocks = int(std::min<uint64_t>((h->n + threads - 1) / threads, uint64_t(h->num_sms) * 32));
+    k_degree_count<<<std::max(blocks, 1), threads, 0, h->stream>>>(dev_graph(h), h->d_deg, d_itv, h->d_err);
     check(h, cudaGetLastError(), "degree kernel launch");
   }
   lpa_status st = take_device_error(h);
@@ -264,6 +261,9 @@ static void build_plan(lpa_handle *h) {
   h->h_deg.resize(h->n);
   check(h, cudaMemcpy(h->h_deg.data(), h->d_deg, h->n * sizeof(uint32_t), cudaMemcpyDeviceToHost),
         "read degrees");
+  std::vector<uint32_t> itv(h->n);
+  check(h, cudaMemcpy(itv.data(), d_itv, h->n * sizeof(uint32_t), cudaMemcpyDeviceToHost), "read interval counts");
+  cudaFree(d_itv);
   h->m = 0;
   h->max_deg = 0;
   for (uint64_t p = 0; p < h->n; p++) {
@@ -271,11 +271,23 @@ static void build_plan(lpa_handle *h) {
     h->max_deg = std::max<uint64_t>(h->max_deg, h->h_deg[p]);
   }
   build_segments(h);
+  for (auto &sg : h->segs) {
+    uint64_t iv = 0;
+    for (uint32_t p = sg.begin; p < sg.end; p++) iv += itv[p];
+    sg.intervals = uint32_t(std::min<uint64_t>(iv, 0xFFFFFFFFull));
+  }
   h->fixed.resize(h->segs.size());
   for (size_t s = 0; s < h->segs.size(); s++) h->fixed[s] = uint8_t(fixed_variant(h->segs[s]));
   std::vector<Seg> ds(h->segs.size());
   for (size_t s = 0; s < h->segs.size(); s++) ds[s] = Seg{h->segs[s].begin, h->segs[s].end};
   h->d_segs = dalloc<Seg>(h, ds.size(), "segments");
+  h->d_seg_var = dalloc<uint8_t>(h, ds.size(), "segment variants");
+  h->d_seg_changed = dalloc<uint32_t>(h, ds.size(), "segment changed counts");
+  h->d_seg_changed_prev = dalloc<uint32_t>(h, ds.size(), "segment changed counts");
+  check(h, cudaMemsetAsync(h->d_seg_changed, 0, std::max<size_t>(1, ds.size()) * sizeof(uint32_t), h->stream),
+        "clear segment counts");
+  check(h, cudaMemsetAsync(h->d_seg_changed_prev, 0, std::max<size_t>(1, ds.size()) * sizeof(uint32_t), h->stream),
+        "clear segment counts");
   h2d(h, h->d_segs, ds.data(), ds.size(), "upload segments");
   check(h, cudaStreamSynchronize(h->stream), "upload segments");
   h->d_seg_cycles = dalloc<long long>(h, h->segs.size(), "segment cycles");
@@ -292,8 +304,9 @@ static void build_plan(lpa_handle *h) {
   if (big) {
     h->gtab_slots = next_pow2_host(2 * big);
     const uint64_t per_block = uint64_t(h->gtab_slots) * 2 * sizeof(uint32_t);
-    h->gtab_blocks = int(std::max<uint64_t>(
-        1, std::min<uint64_t>(uint64_t(h->num_sms) * h->occ_block, (1ull << 30) / per_block)));
+    // one table per block of the persistent kernel; at most 2 GiB of tables
+    h->gtab_blocks = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(h->grid), (2ull << 30) / per_block)));
+    h->grid = std::min(h->grid, h->gtab_blocks);
     h->d_gtab = dalloc<uint32_t>(h, uint64_t(h->gtab_blocks) * 2 * h->gtab_slots, "global count tables");
     check(h, cudaMemsetAsync(h->d_gtab, 0, uint64_t(h->gtab_blocks) * per_block, h->stream), "clear tables");
   }
@@ -301,7 +314,7 @@ static void build_plan(lpa_handle *h) {
                  h->opts.force_variant);
 }
 
-static IterArgs iter_args(lpa_handle *h, int list, unsigned long long *changed) {
+static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *work) {
   IterArgs a{};
   a.g = dev_graph(h);
   a.labs0 = h->d_lab[0];
@@ -309,60 +322,42 @@ static IterArgs iter_args(lpa_handle *h, int list, unsigned long long *changed) 
   a.parity0 = uint32_t(h->cur);
   a.it_dev = h->loop_it;
   a.changed = changed;
+  a.work = work;
   a.err = h->d_err;
   a.segs = h->d_segs;
-  a.seg_list = h->d_lists + h->list_off[list];
-  a.n_list = h->list_off[list + 1] - h->list_off[list];
-  a.seg_cycles = h->opts.record_timings ? h->d_seg_cycles : nullptr;
+  a.seg_var = h->d_seg_var;
+  a.heavy = h->d_lists;
+  a.n_heavy = h->n_heavy;
+  a.light = h->d_lists + h->n_heavy;
+  a.n_light = h->n_light;
+  a.two_pass = h->d_lists + h->n_heavy + h->n_light;
+  a.n_two_pass = h->n_two_pass;
+  a.seg_cycles = (h->opts.record_timings >= 2 || h->collect_cycles) ? h->d_seg_cycles : nullptr;
+  a.seg_changed = h->learner ? h->d_seg_changed : nullptr;
   a.cms_thr = h->opts.cms_threshold;
   for (int r = 0; r < kCmsDepth; r++) a.seeds[r] = h->seeds[r];
   a.scratch = h->d_scratch;
   a.arc_off = h->d_arc_off;
-  a.from_scratch = (list == kListTwoLight || list == kListTwoHeavy) ? 1 : 0;
   a.gtab = h->d_gtab;
   a.gtab_slots = h->gtab_slots;
   return a;
 }
 
-constexpr size_t kSmemPacked = size_t(kLaneWarps) * kStage * sizeof(uint32_t);
-constexpr size_t kSmemWarp = size_t(kLaneWarps) * (kStage + 2 * kV1Slots) * sizeof(uint32_t);
-constexpr size_t kSmemBlock = size_t(2) * kBlockSlots * sizeof(uint32_t);
-
-// Enqueues one iteration (no host synchronisation).  Swaps the buffers.
-static void enqueue_iteration(lpa_handle *h, unsigned long long *changed) {
+// Enqueues one iteration (no host synchronisation).  Swaps the buffers.  The
+// changed counter and the two queue counters of the iteration's slot must be
+// zero.
+static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32_t *work) {
   const bool timed = h->opts.record_timings && h->events_ready;
-  auto launch = [&](int list, auto body) {
-    if (h->list_off[list + 1] == h->list_off[list]) return;
-    if (timed) cudaEventRecord(h->ev[2 * list], h->stream);
-    body(iter_args(h, list, changed));
+  const IterArgs a = iter_args(h, changed, work);
+  if (timed) cudaEventRecord(h->ev[0], h->stream);
+  if (h->n_two_pass) {
+    k_decode_two_pass<<<h->grid_decode, kThreads, 0, h->stream>>>(a);
     h->launches++;
-    if (timed) cudaEventRecord(h->ev[2 * list + 1], h->stream);
-  };
-  if (timed) cudaEventRecord(h->ev[2 * kNumLists], h->stream);
-  launch(kListPacked, [&](const IterArgs &a) {
-    k_lane_batch_packed<<<h->grid[kListPacked], kLaneWarps * 32, kSmemPacked, h->stream>>>(a);
-  });
-  launch(kListWarp, [&](const IterArgs &a) {
-    k_lane_batch_warp<<<h->grid[kListWarp], kLaneWarps * 32, kSmemWarp, h->stream>>>(a);
-  });
-  launch(kListBlock, [&](const IterArgs &a) {
-    k_block<<<h->grid[kListBlock], kBlockThreads, kSmemBlock, h->stream>>>(a);
-  });
-  if (h->v4_all_n) {
-    IterArgs a = iter_args(h, kListTwoLight, changed);
-    a.seg_list = h->d_lists + h->v4_all_off;
-    a.n_list = h->v4_all_n;
-    if (timed) cudaEventRecord(h->ev[2 * kListTwoLight], h->stream);
-    k_decode_segments<<<h->grid_decode, 256, 0, h->stream>>>(a);
-    h->launches++;
-    launch(kListTwoLight, [&](const IterArgs &b) {
-      k_lane_batch_warp<<<h->grid[kListTwoLight], kLaneWarps * 32, kSmemWarp, h->stream>>>(b);
-    });
-    launch(kListTwoHeavy, [&](const IterArgs &b) {
-      k_block<<<h->grid[kListTwoHeavy], kBlockThreads, kSmemBlock, h->stream>>>(b);
-    });
   }
-  if (timed) cudaEventRecord(h->ev[2 * kNumLists + 1], h->stream);
+  if (timed) cudaEventRecord(h->ev[1], h->stream);
+  k_iterate<<<h->grid, kThreads, kSmemBytes, h->stream>>>(a);
+  h->launches++;
+  if (timed) cudaEventRecord(h->ev[2], h->stream);
   h->cur ^= 1;
 }
 
@@ -377,17 +372,9 @@ static void collect_times(lpa_handle *h) {
     return double(t);
   };
   for (int v = 0; v < 4; v++) h->variant_ms[v] = 0;
-  if (h->list_off[kListWarp + 1] > h->list_off[kListWarp])
-    h->variant_ms[LPA_VARIANT_WARP] = ms(2 * kListWarp, 2 * kListWarp + 1);
-  if (h->list_off[kListPacked + 1] > h->list_off[kListPacked])
-    h->variant_ms[LPA_VARIANT_PACKED] = ms(2 * kListPacked, 2 * kListPacked + 1);
-  if (h->list_off[kListBlock + 1] > h->list_off[kListBlock])
-    h->variant_ms[LPA_VARIANT_BLOCK] = ms(2 * kListBlock, 2 * kListBlock + 1);
-  if (h->v4_all_n) {
-    const int last = (h->list_off[kListTwoHeavy + 1] > h->list_off[kListTwoHeavy]) ? kListTwoHeavy : kListTwoLight;
-    h->variant_ms[LPA_VARIANT_TWO_PASS] = ms(2 * kListTwoLight, 2 * last + 1);
-  }
-  h->last_iter_ms = ms(2 * kNumLists, 2 * kNumLists + 1);
+  h->decode_ms = ms(0, 1);
+  h->iterate_ms = ms(1, 2);
+  h->last_iter_ms = ms(0, 2);
 }
 
 // ------------------------------------------------------------------ C ABI --
@@ -448,6 +435,7 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
   if (!h) return LPA_ERR_OOM;
   if (o) h->opts = *o;
   else lpa_opts_default(&h->opts);
+  if (h->opts.dispatch == LPA_DISPATCH_LEARNED && h->opts.record_timings < 1) h->opts.record_timings = 1;
   try {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -465,20 +453,11 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
       check(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
       h->own_stream = true;
     }
-    check(h, cudaFuncSetAttribute(k_lane_batch_packed, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemPacked)),
+    check(h, cudaFuncSetAttribute(k_iterate, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)),
           "smem attr");
-    check(h, cudaFuncSetAttribute(k_lane_batch_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemWarp)),
-          "smem attr");
-    check(h, cudaFuncSetAttribute(k_block, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBlock)), "smem attr");
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ_packed, k_lane_batch_packed, kLaneWarps * 32,
-                                                           kSmemPacked), "occupancy");
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ_warp, k_lane_batch_warp, kLaneWarps * 32,
-                                                           kSmemWarp), "occupancy");
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ_block, k_block, kBlockThreads, kSmemBlock),
-          "occupancy");
-    h->occ_packed = std::max(1, h->occ_packed);
-    h->occ_warp = std::max(1, h->occ_warp);
-    h->occ_block = std::max(1, h->occ_block);
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ, k_iterate, kThreads, kSmemBytes), "occupancy");
+    h->occ = std::max(1, h->occ);
+    h->grid = h->num_sms * h->occ;
 
     h->n = n;
     h->n_c = n_c;
@@ -504,6 +483,9 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     h->d_lab[1] = dalloc<uint32_t>(h, n, "labels");
     h->changed_slots = kMaxRunSlots;
     h->d_changed = dalloc<unsigned long long>(h, h->changed_slots, "changed counters");
+    h->d_work = dalloc<uint32_t>(h, 2 * size_t(h->changed_slots), "work counters");
+    check(h, cudaMemsetAsync(h->d_work, 0, 2 * size_t(h->changed_slots) * sizeof(uint32_t), h->stream),
+          "clear work counters");
     check(h, cudaMemsetAsync(h->d_changed, 0, h->changed_slots * sizeof(unsigned long long), h->stream),
           "clear counters");
     h->d_err = dalloc<uint32_t>(h, 1, "error word");
@@ -608,7 +590,8 @@ lpa_status lpa_iterate(lpa_handle *h, uint64_t *changed_out) {
     lpa_learner_before_iteration(h);
     unsigned long long *slot = h->d_changed;
     check(h, cudaMemsetAsync(slot, 0, sizeof(unsigned long long), h->stream), "clear counter");
-    enqueue_iteration(h, slot);
+    check(h, cudaMemsetAsync(h->d_work, 0, 2 * sizeof(uint32_t), h->stream), "clear work counters");
+    enqueue_iteration(h, slot, h->d_work);
     check(h, cudaGetLastError(), "iteration launch");
     check(h, cudaMemcpyAsync(h->h_pinned, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream),
           "read counter");
@@ -633,7 +616,21 @@ lpa_status lpa_iterate(lpa_handle *h, uint64_t *changed_out) {
 lpa_status lpa_run(lpa_handle *h, int max_iter, int early_exit, int *iters_done) {
   if (!h || max_iter < 0) return LPA_ERR_INVALID_ARG;
   if (iters_done) *iters_done = 0;
-  return lpa_run_graph(h, max_iter, early_exit != 0, iters_done);
+  int done = 0;
+  while (done < max_iter && !lpa_learner_settled(h)) {  // the cost model learns on host-driven iterations
+    uint64_t ch = 0;
+    lpa_status st = lpa_iterate(h, &ch);
+    if (st != LPA_OK) return st;
+    done++;
+    if (early_exit && ch == 0) {
+      if (iters_done) *iters_done = done;
+      return LPA_OK;
+    }
+  }
+  int rest = 0;
+  lpa_status st = lpa_run_graph(h, max_iter - done, early_exit != 0, &rest);
+  if (iters_done) *iters_done = done + rest;
+  return st;
 }
 
 lpa_status lpa_get_changed_history(lpa_handle *h, uint64_t *out, size_t count) {
@@ -663,6 +660,8 @@ lpa_status lpa_get_stats(lpa_handle *h, lpa_stats *st) {
   st->last_changed = h->last_changed;
   st->last_iter_ms = h->last_iter_ms;
   st->launches = h->launches;
+  st->decode_ms = h->decode_ms;
+  st->iterate_ms = h->iterate_ms;
   for (int v = 0; v < 4; v++) st->variant_ms[v] = h->variant_ms[v];
   for (size_t s = 0; s < h->segs.size(); s++) {
     st->variant_segments[h->variant[s]]++;
@@ -727,6 +726,7 @@ lpa_status lpa_set_dispatch(lpa_handle *h, int dispatch, int force_variant) {
     check(h, cudaSetDevice(h->device), "cudaSetDevice");
     h->opts.dispatch = dispatch;
     h->opts.force_variant = force_variant;
+    if (dispatch == LPA_DISPATCH_LEARNED && h->opts.record_timings < 1) h->opts.record_timings = 1;
     lpa_learner_reset(h);
     apply_dispatch(h, dispatch == LPA_DISPATCH_FORCE ? LPA_DISPATCH_FORCE : LPA_DISPATCH_FIXED, force_variant);
     check(h, cudaStreamSynchronize(h->stream), "dispatch");
@@ -751,7 +751,9 @@ lpa_status lpa_get_segments(lpa_handle *h, uint32_t *begin, uint32_t *end, uint8
 }  // extern "C"
 
 // Internal hooks used by the dispatch and graph-loop modules.
-void lpa_rt_enqueue_iteration(lpa_handle *h, unsigned long long *changed) { enqueue_iteration(h, changed); }
+void lpa_rt_enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32_t *work) {
+  enqueue_iteration(h, changed, work);
+}
 void lpa_rt_apply_variants(lpa_handle *h) {
   bool any_two = false;
   for (auto v : h->variant) any_two |= v == LPA_VARIANT_TWO_PASS;

@@ -16,10 +16,6 @@ namespace lpa_rt {
 // for vertices only the block and two-pass variants can take).
 enum Bucket : uint8_t { kTiny = 0, kMid = 1, kLarge = 2, kHeavy = 3, kNumBuckets = 4 };
 
-// Launch lists: one per variant, the two-pass variant split by the kernel
-// that counts its segments.
-enum List : int { kListWarp = 0, kListPacked = 1, kListBlock = 2, kListTwoLight = 3, kListTwoHeavy = 4,
-                  kNumLists = 5 };
 
 struct SegInfo {
   uint32_t begin, end;
@@ -75,12 +71,16 @@ struct lpa_handle {
   std::vector<uint8_t> variant;  // per segment
   std::vector<uint8_t> fixed;    // per segment, the heuristic's choice
   lpa_dev::Seg *d_segs = nullptr;
-  uint32_t *d_lists = nullptr;
-  uint32_t list_off[lpa_rt::kNumLists + 1] = {0};
-  uint32_t v4_all_off = 0, v4_all_n = 0;  // two-pass segments (both lists) for pass 1
-  int grid[lpa_rt::kNumLists] = {0};
-  int grid_decode = 0;
-  int occ_packed = 1, occ_warp = 1, occ_block = 1;
+  uint8_t *d_seg_var = nullptr;
+  uint32_t *d_lists = nullptr;  // heavy items | light chunk items | two-pass segments
+  uint32_t n_heavy = 0, n_light = 0, n_two_pass = 0;
+  size_t lists_cap = 0;
+  int grid = 0;          // persistent iteration kernel
+  int grid_decode = 0;   // two-pass decode kernel
+  int occ = 1;
+  uint32_t *d_work = nullptr;        // two queue counters per iteration slot
+  uint32_t *d_seg_changed = nullptr; // per-segment changed counts (cost-model feature)
+  uint32_t *d_seg_changed_prev = nullptr;  // the previous iteration's
 
   // scratch
   uint64_t *d_arc_off = nullptr;
@@ -97,7 +97,9 @@ struct lpa_handle {
   std::vector<uint64_t> history;
   double last_iter_ms = 0;
   double variant_ms[4] = {0, 0, 0, 0};
-  cudaEvent_t ev[2 * lpa_rt::kNumLists + 2] = {};
+  double decode_ms = 0, iterate_ms = 0;
+  bool collect_cycles = false;  // per-segment cycles for the cost model
+  cudaEvent_t ev[4] = {};  // two-pass decode start/end, iteration start/end
   bool events_ready = false;
   uint64_t device_bytes = 0;
   std::vector<void *> allocations;
@@ -122,6 +124,7 @@ void lpa_learner_reset(lpa_handle *h);
 void lpa_learner_before_iteration(lpa_handle *h);
 void lpa_learner_after_iteration(lpa_handle *h);
 void lpa_learner_stats(lpa_handle *h, lpa_stats *st);
-void lpa_rt_enqueue_iteration(lpa_handle *h, unsigned long long *changed);
+bool lpa_learner_settled(lpa_handle *h);
+void lpa_rt_enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32_t *work);
 void lpa_rt_apply_variants(lpa_handle *h);
 lpa_status lpa_rt_take_error(lpa_handle *h);
