@@ -229,7 +229,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat-s24", choices=sorted(WORKLOADS))
-    ap.add_argument("--dispatch", default="fixed", choices=["fixed", "learned"])
+    ap.add_argument("--dispatch", default="learned", choices=["fixed", "learned"],
+                    help="learned: the MLP plan (judged against the fixed buckets, also measured)")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -257,8 +258,7 @@ def main():
     arr = shared_graph_arrays(args.workload, w, rank, world, device)
     stream = torch.cuda.Stream(device=device)
     p = L.Propagator(L.desc_from_arrays(arr), device=local, cms_threshold=w["cms"], cms_seed=1,
-                     record_timings=1, stream=stream.cuda_stream,
-                     dispatch=L.Dispatch.FIXED)
+                     record_timings=1, stream=stream.cuda_stream, dispatch=L.Dispatch.FIXED)
     info = p.get_info()
     arcs = int(info.num_arcs)
     b_alg = int(info.bytes_algorithmic)
@@ -266,26 +266,47 @@ def main():
     flush = inputs_bytes < 2 * L2_BYTES
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=device) if flush else None
 
-    # warm-up
+    def timed_region(steps):
+        """K iterations; device time of each from the library's CUDA events."""
+        dev = 0.0
+        kern = np.zeros(2)
+        for _ in range(steps):
+            if flush:
+                with torch.cuda.stream(stream):
+                    flush_buf.fill_(1)
+            p.iterate()
+            s = p.stats()
+            dev += s.last_iter_ms
+            kern += np.array([s.decode_ms, s.iterate_ms])
+        return dev, kern
+
+    # fixed degree-bucket plan (the reference's buckets): warm-up then timed
     p.init_labels()
     for _ in range(args.warmup):
         p.iterate()
+    barrier(world, device)
+    torch.cuda.synchronize()
+    fixed_ms, _ = timed_region(args.steps)
+    fixed_ms = max_over_ranks(fixed_ms, world, device)
+    learned_info = None
+    if args.dispatch == "learned":
+        # the cost model explores and trains on warm-up iterations, then its plan is timed
+        p.set_dispatch(L.Dispatch.LEARNED)
+        p.init_labels()
+        for _ in range(max(args.warmup, 8)):
+            p.iterate()
+        ls = p.stats()
+        learned_info = {"active": int(ls.learned_active), "mlp_updates": int(ls.mlp_updates),
+                        "mlp_loss": float(ls.mlp_loss), "reverts": int(ls.dispatch_reverts),
+                        "segments_per_variant": [int(x) for x in ls.variant_segments],
+                        "arcs_per_variant": [int(x) for x in ls.variant_arcs]}
 
     st0 = p.stats()
     barrier(world, device)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     wall0 = time.perf_counter()
-    dev_ms = 0.0
-    kern_ms = np.zeros(2)
-    for _ in range(args.steps):
-        if flush:
-            with torch.cuda.stream(stream):
-                flush_buf.fill_(1)
-        p.iterate()
-        s = p.stats()
-        dev_ms += s.last_iter_ms
-        kern_ms += np.array([s.decode_ms, s.iterate_ms])
+    dev_ms, kern_ms = timed_region(args.steps)
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     clk = clocks.stop()
@@ -346,6 +367,11 @@ def main():
                          "traffic": traffic_summary(args.workload),
                          "iteration": {"bytes": b_alg, "achieved": iter_achieved, "frac": iter_achieved / peak},
                          "kernel_ms": {"k_decode_two_pass": float(kern_avg[0]), "k_iterate": float(kern_avg[1])}},
+            "dispatch": {"mode": args.dispatch,
+                         "fixed_value": arcs * args.steps * world / (fixed_ms / 1e3),
+                         "fixed_ms_per_step": fixed_ms / args.steps,
+                         "learned_over_fixed": (fixed_ms / total_ms) if args.dispatch == "learned" else None,
+                         "learner": learned_info},
             "cpu_baseline": cb,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * arr["n"],
                     "d2h_bytes_per_step": 4 * arr["n"] + 8},

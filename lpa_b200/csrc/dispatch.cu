@@ -14,8 +14,8 @@
 //      ((s + k) mod capable)-th capable variant) -- every step trains the MLP;
 //   3. the MLP's plan runs; if its iteration is slower than the fixed plan's,
 //      the handle reverts to the fixed plan (a revert is counted);
-//   4. every kRecheck iterations one fixed iteration refreshes the reference
-//      and the comparison is repeated.
+//   4. the chosen plan stays frozen; every kRecheck iterations one iteration
+//      runs the other plan and the faster of the two is kept.
 // Features: degree, compressed bits, interval fraction, residual count (per
 // vertex of the segment), iteration index and the segment's change rate in
 // the previous iteration.
@@ -395,8 +395,6 @@ void lpa_learner_after_iteration(lpa_handle *h) {
       } else {
         if (fixed_now) L->t_fixed = t;
         else L->t_learned = t;
-        if (!fixed_now) train(h);
-        if (L->phase == kPhaseLearned && !fixed_now) infer(h);
         L->since_check++;
       }
       break;

@@ -131,24 +131,6 @@ struct CmsBestSink {
   }
 };
 
-// Labels of stage[0..total) in place (ids -> labels), 4 loads in flight per thread.
-__device__ __forceinline__ void block_gather_inplace(uint32_t *stage, uint32_t total,
-                                                     const uint32_t *__restrict__ lab_in) {
-  for (uint32_t k0 = threadIdx.x; k0 < total; k0 += 4 * kThreads) {
-    uint32_t v[4];
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const uint32_t k = k0 + u * kThreads;
-      v[u] = k < total ? __ldg(lab_in + stage[k]) : 0u;
-    }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const uint32_t k = k0 + u * kThreads;
-      if (k < total) stage[k] = v[u];
-    }
-  }
-}
-
 // Labels of the global ids src[0..total) into stage.
 __device__ __forceinline__ void block_gather_from(uint32_t *stage, const uint32_t *__restrict__ src, uint32_t total,
                                                   const uint32_t *__restrict__ lab_in) {
@@ -194,7 +176,7 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
       block_consume_stage(stage, cnt, sink);
       __syncthreads();
     }
-    return d <= kStage;
+    return false;
   }
   const uint64_t end = g.offsets[p + 1];
   bool bad = false;
@@ -275,7 +257,9 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
     if (has && j == nseg_i - 1) sh.last_end = r.pos;
   }
   __syncthreads();
-  // ---- residual section: rounds of up to kResSegChunk segments staged in shared memory
+  // ---- residual section: every warp walks its own 256-bit segments (lane per
+  // segment, 32 per round) through its slice of the staging area; warps only
+  // meet again at the end.
   if (t == 0) {
     BitReader r;
     r.seek(g.words, sh.last_end);
@@ -291,56 +275,99 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
   __syncthreads();
   const uint32_t nseg_r = sh.nseg_r;
   const uint64_t rbase = sh.rbase;
-  for (uint32_t j0 = 0; j0 < nseg_r; j0 += kResSegChunk) {
-    const uint32_t j = j0 + t;
-    bool has = t < kResSegChunk && j < nseg_r;
+  const uint32_t lane = t & 31u, warp = t >> 5;
+  uint32_t *wst = stage + warp * kWarpStage;
+  bool single = true;  // this warp's labels all sit in its slice after one batch
+  uint32_t staged = 0;
+  int batches = 0;
+  for (uint32_t j0 = warp * 32u; j0 < nseg_r; j0 += kWarps * 32u) {
+    const uint32_t j = j0 + lane;
+    bool has = j < nseg_r;
     BitReader r;
     uint32_t cnt = 0;
-    const uint64_t q = rbase + uint64_t(kSegBits) * j;
     if (has) {
+      const uint64_t q = rbase + uint64_t(kSegBits) * j;
       if (q >= end) {
         bad = true;
         has = false;
       } else {
         r.seek(g.words, q);
         cnt = r.gamma(bad);
-        if (bad || cnt > kStage) {
+        if (bad || cnt > kWarpStage) {
           bad = true;
           cnt = 0;
         }
       }
     }
-    const uint32_t total = block_scan(sh, cnt);
-    if (total > kStage) {  // more items than a round of well-formed segments can hold
-      if (t == 0) sh.bad = 1;
-      __syncthreads();
-      break;
-    }
-    if (has) {
-      uint32_t o = sh.pref[t], v = 0;
-      for (uint32_t cc = 0; cc < cnt; cc++) {
-        const uint32_t x = r.zeta3(bad);
-        v = (cc == 0) ? zigzag_first(node, x) : v + x + 1u;
-        if (bad || r.pos > end || uint64_t(v) >= g.n) {
-          bad = true;
-          v = node;  // keeps the staged id in range; the error word reports the stream
+    uint32_t done = ~__ballot_sync(kFull, has);
+    while (done != kFull) {
+      const bool pending = !((done >> lane) & 1u);
+      const uint32_t sc = pending ? cnt : 0u;
+      const uint32_t incl = warp_incl_scan(sc, lane);
+      const bool in_batch = pending && incl <= kWarpStage;
+      const uint32_t batch = __ballot_sync(kFull, in_batch);
+      const uint32_t total = __shfl_sync(kFull, incl, 31 - __clz(batch));
+      if (in_batch) {
+        uint32_t o = incl - sc, v = 0;
+        for (uint32_t cc = 0; cc < cnt; cc++) {
+          const uint32_t x = r.zeta3(bad);
+          v = (cc == 0) ? zigzag_first(node, x) : v + x + 1u;
+          if (bad || r.pos > end || uint64_t(v) >= g.n) {
+            bad = true;
+            v = node;  // keeps the staged id in range; the error word reports the stream
+          }
+          wst[o++] = v;
         }
-        stage[o++] = v;
+        my_items += cnt;
+        if (j == nseg_r - 1) sh.last_end = r.pos;
       }
-      my_items += cnt;
-      if (j == nseg_r - 1) sh.last_end = r.pos;
+      __syncwarp();
+      for (uint32_t k0 = lane; k0 < total; k0 += 256) {
+        uint32_t lv[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const uint32_t k = k0 + 32 * u;
+          lv[u] = k < total ? __ldg(c.lab_in + wst[k]) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const uint32_t k = k0 + 32 * u;
+          if (k < total) wst[k] = lv[u];
+        }
+      }
+      __syncwarp();
+      for (uint32_t k0 = 0; k0 < total; k0 += 32) {
+        const uint32_t k = k0 + lane;
+        const bool ok = k < total;
+        sink(ok, ok ? wst[k] : 0u);
+      }
+      __syncwarp();
+      staged = total;
+      batches++;
+      done |= batch;
     }
-    __syncthreads();
-    block_gather_inplace(stage, total, c.lab_in);
-    __syncthreads();
-    block_consume_stage(stage, total, sink);
-    __syncthreads();
   }
+  if (batches > 1) single = false;
   if (my_items) atomicAdd(&sh.items, my_items);
   if (bad) sh.bad = 1;
-  __syncthreads();
+  const bool all_single = __syncthreads_and(single) != 0;
   if (t == 0 && (sh.bad || sh.last_end != end || sh.items != d)) set_error(a.err, kErrBadStream);
-  return nseg_i == 0 && nseg_r <= kResSegChunk;
+  if (lane == 0) sh.wsum[warp] = staged;
+  __syncthreads();
+  return nseg_i == 0 && all_single;
+}
+
+// Second pass over labels left in the warps' slices by heavy_produce.
+template <class Sink>
+__device__ __forceinline__ void heavy_consume_staged(BlockSh &sh, const uint32_t *stage, const Sink &sink) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t *wst = stage + warp * kWarpStage;
+  const uint32_t total = sh.wsum[warp];
+  for (uint32_t k0 = 0; k0 < total; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    const bool ok = k < total;
+    sink(ok, ok ? wst[k] : 0u);
+  }
 }
 
 // One heavy vertex by the whole block.
@@ -358,7 +385,8 @@ __device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint3
     const bool staged = heavy_produce(a, c, sh, stage, p, node, d, from_scratch, CmsAddSink{cms, a.seeds});
     __syncthreads();
     CmsBestSink s2{cms, a.seeds, &best};
-    if (staged) block_consume_stage(stage, d, s2);
+    if (staged) heavy_consume_staged(sh, stage, s2);
+    else if ((p >= g.n_c || from_scratch) && d <= kStage) block_consume_stage(stage, d, s2);
     else heavy_produce(a, c, sh, stage, p, node, d, from_scratch, s2);
     __syncthreads();
     for (uint32_t i = t; i < kCmsDepth * kCmsWidth; i += kThreads) cms[i] = 0u;
@@ -402,12 +430,149 @@ __device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint3
   __syncthreads();
 }
 
+// Decodes the compressed vertices of a warp batch into stage (ids).  Lane l
+// owns the batch vertex in lane l: it reads that vertex's section headers and
+// writes its interval items (lane per vertex); then the batch's residual
+// segments are spread over the lanes (lane per 256-bit segment, 32 per
+// round) and placed with warp prefix sums over the segments' item counts.
+// Returns false (after filling every region with in-range ids) on a
+// malformed stream.
+__device__ bool warp_decode_batch(const DevGraph &g, uint32_t *stage, bool active, uint32_t p, uint32_t node,
+                                  uint32_t d, uint32_t base, uint32_t lane) {  // stage: shared or global
+  bool bad = false;
+  uint32_t nres = 0, itv = 0;
+  uint64_t rbase = 0, end = 0;
+  if (active && d) {
+    end = g.offsets[p + 1];
+    BitReader r;
+    r.seek(g.words, g.offsets[p]);
+    uint32_t ns = r.segcnt(bad);
+    const uint64_t ib = r.pos;
+    uint64_t last = r.pos;
+    if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
+      bad = true;
+      ns = 0;
+    }
+    for (uint32_t j = 0; j < ns && !bad; j++) {
+      const uint64_t q = ib + uint64_t(kSegBits) * j;
+      if (q >= end) {
+        bad = true;
+        break;
+      }
+      if (j) r.seek(g.words, q);
+      const uint32_t cnt = r.gamma(bad);
+      uint32_t left = 0;
+      for (uint32_t c = 0; c < cnt && !bad; c++) {
+        const uint32_t l = r.gamma(bad);
+        left = (c == 0) ? zigzag_first(node, l) : left + l + 1u;
+        const uint32_t len = r.gamma(bad) + kMinItv;
+        if (bad || r.pos > end || uint64_t(left) + len > g.n || uint64_t(itv) + len > d) {
+          bad = true;
+          break;
+        }
+        for (uint32_t k = 0; k < len; k++) stage[base + itv + k] = left + k;
+        itv += len;
+        left += len;
+      }
+      last = r.pos;
+    }
+    if (ns) r.seek(g.words, last);
+    if (!bad) {
+      nres = r.segcnt(bad);
+      rbase = r.pos;
+      if (bad || r.pos > end || nres > (end - r.pos) / kSegBits + 1) {
+        bad = true;
+        nres = 0;
+      } else if (nres == 0 && r.pos != end) {
+        bad = true;
+      }
+    }
+  }
+  const uint32_t seg_incl = warp_incl_scan(nres, lane);
+  const uint32_t seg_excl = seg_incl - nres;
+  const uint32_t S = __shfl_sync(kFull, seg_incl, 31);
+  uint32_t res_done = 0;
+  for (uint32_t r0 = 0; r0 < S; r0 += 32) {
+    const uint32_t f = r0 + lane;
+    const bool has = f < S;
+    // owner: the last lane whose first segment is <= f
+    uint32_t lo = 0, hi = 31;
+#pragma unroll
+    for (int step = 0; step < 5; step++) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      const uint32_t e = __shfl_sync(kFull, seg_excl, mid);
+      if (e <= f) lo = mid;
+      else hi = mid - 1;
+    }
+    const uint32_t o = lo;
+    const uint32_t eo = __shfl_sync(kFull, seg_excl, o);
+    const uint32_t no = __shfl_sync(kFull, nres, o);
+    const uint64_t rb = __shfl_sync(kFull, rbase, o);
+    const uint64_t en = __shfl_sync(kFull, end, o);
+    const uint32_t ndo = __shfl_sync(kFull, node, o);
+    const uint32_t bo = __shfl_sync(kFull, base, o);
+    const uint32_t io = __shfl_sync(kFull, itv, o);
+    const uint32_t dd = __shfl_sync(kFull, d, o);
+    const uint32_t rdo = __shfl_sync(kFull, res_done, o);
+    const uint32_t j = f - eo;
+    BitReader rr;
+    uint32_t cnt = 0;
+    if (has) {
+      const uint64_t q = rb + uint64_t(kSegBits) * j;
+      if (q >= en) {
+        bad = true;
+      } else {
+        rr.seek(g.words, q);
+        cnt = rr.gamma(bad);
+        if (bad || cnt > dd) {
+          bad = true;
+          cnt = 0;
+        }
+      }
+    }
+    const uint32_t c_incl = warp_incl_scan(cnt, lane);
+    const uint32_t c_excl = c_incl - cnt;
+    const uint32_t fo = (eo > r0 ? eo : r0) - r0;  // the owner's first lane in this round
+    const uint32_t at_fo = __shfl_sync(kFull, c_excl, fo);
+    if (has && !bad) {
+      const uint32_t rel = io + rdo + (c_excl - at_fo);  // item offset inside the owner's region
+      uint32_t v = 0;
+      for (uint32_t c = 0; c < cnt; c++) {
+        const uint32_t x = rr.zeta3(bad);
+        v = (c == 0) ? zigzag_first(ndo, x) : v + x + 1u;
+        if (bad || rr.pos > en || uint64_t(v) >= g.n || rel + c >= dd) {
+          bad = true;
+          break;
+        }
+        stage[bo + rel + c] = v;
+      }
+      if (j == no - 1 && rr.pos != en) bad = true;
+    }
+    // owners advance by the items of their segments in this round
+    const uint32_t fv = (seg_excl > r0 ? seg_excl : r0) - r0;
+    const uint32_t lv_end = (seg_incl < r0 + 32 ? seg_incl : r0 + 32);
+    const bool mine = nres && seg_incl > r0 && seg_excl < r0 + 32;
+    const uint32_t lv = mine ? lv_end - r0 - 1 : 0u;
+    const uint32_t a1 = __shfl_sync(kFull, c_incl, lv);
+    const uint32_t a0 = __shfl_sync(kFull, c_excl, mine ? fv : 0u);
+    if (mine) res_done += a1 - a0;
+  }
+  if (active && d && itv + res_done != d) bad = true;
+  if (__any_sync(kFull, bad)) {
+    if (active)
+      for (uint32_t k = 0; k < d; k++) stage[base + k] = node;
+    __syncwarp();
+    return false;
+  }
+  return true;
+}
+
 // Up to 32 consecutive positions [p0, p1) by one warp.
 __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, uint32_t *keys, uint32_t *cnts,
                             uint32_t seg, uint32_t p0, uint32_t p1, int variant, unsigned long long &changed) {
   const DevGraph &g = a.g;
   const uint32_t lane = threadIdx.x & 31u;
-  constexpr uint32_t cap_stage = kStage / kWarps;
+  constexpr uint32_t cap_stage = kWarpStage;
   const uint32_t p = p0 + lane;
   const bool valid = p < p1;
   const uint32_t node = valid ? g.vertices[p] : 0u;
@@ -434,18 +599,9 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, ui
     const uint32_t lo = __ffs(batch) - 1, hi = 32 - __clz(batch);
     const uint32_t total = __shfl_sync(kFull, incl, hi - 1);
     const uint32_t base = incl - sd;
-    // 1. ids (decoded lane-per-vertex)
-    if (decode && in_batch && d) {
-      uint32_t k = 0;
-      const int64_t r = walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], node, g.n, [&](uint32_t id) {
-        if (k < d) stage[base + k] = id;
-        k++;
-      });
-      if (r != int64_t(d)) {
-        set_error(a.err, kErrBadStream);
-        for (uint32_t q = (r > 0 ? uint32_t(r) : 0u); q < d; q++) stage[base + q] = node;
-      }
-    }
+    // 1. ids: the batch decoded by all lanes together
+    if (decode && !warp_decode_batch(g, stage, in_batch, p, node, d, base, lane) && lane == 0)
+      set_error(a.err, kErrBadStream);
     __syncwarp();
     // 2. labels: every load of the batch in flight together
     for (uint32_t k0 = lane; k0 < total; k0 += 128) {
@@ -506,7 +662,7 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, ui
           const uint32_t maxc = __reduce_max_sync(kFull, cnt);
           bestl = __reduce_min_sync(kFull, (ok && cnt == maxc) ? lab : kFull);
         } else {
-          const uint32_t cap = next_pow2(2 * dv);
+          const uint32_t cap = min(next_pow2(2 * dv), kWarpSlots);  // > dv: every label fits
           for (uint32_t k0 = 0; k0 < dv; k0 += 32) {
             const uint32_t k = k0 + lane;
             const bool ok = k < dv;
@@ -548,7 +704,7 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, ui
 
 }  // namespace
 
-__global__ void __launch_bounds__(kThreads, 3) k_iterate(IterArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
   extern __shared__ uint32_t smem[];
   __shared__ BlockSh sh;
   uint32_t *stage = smem;         // kStage words
@@ -580,7 +736,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_iterate(IterArgs a) {
   // light chunks: one warp per chunk of up to 32 positions
   uint32_t *wkeys = tab + warp * kWarpSlots;
   uint32_t *wcnts = tab + kTableSlots + warp * kWarpSlots;
-  uint32_t *wstage = stage + warp * (kStage / kWarps);
+  uint32_t *wstage = stage + warp * kWarpStage;
   for (;;) {
     uint32_t i = 0;
     if (lane == 0) i = atomicAdd(qctr + 1, 1u);
@@ -598,32 +754,164 @@ __global__ void __launch_bounds__(kThreads, 3) k_iterate(IterArgs a) {
   flush_changed(c.changed, changed);
 }
 
-// Two-pass variant, pass 1: decode the two-pass segments' compressed positions
-// into the scratch CSR (block per segment, thread per position).
+// Two-pass variant, pass 1: the two-pass segments' compressed positions are
+// decoded into the scratch CSR.  Light segments: one warp per 32-position
+// chunk with the segment-parallel warp decoder.  Single hub vertices: the
+// block decodes 256 residual segments per round (one thread each) at offsets
+// from a block prefix sum, after expanding the interval section.
 __global__ void __launch_bounds__(kThreads) k_decode_two_pass(IterArgs a) {
+  __shared__ BlockSh sh;
   const DevGraph &g = a.g;
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   for (uint32_t i = blockIdx.x; i < a.n_two_pass; i += gridDim.x) {
     const uint32_t s = a.two_pass[i];
     const Seg sg = a.segs[s];
     if (sg.begin >= g.n_c) continue;
     const long long t0 = clock64();
-    for (uint32_t p = sg.begin + threadIdx.x; p < sg.end; p += kThreads) {
-      uint32_t *dst = a.scratch + a.arc_off[p];
-      const uint32_t d = g.deg[p];
-      uint32_t k = 0;
-      const int64_t r = walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], g.vertices[p], g.n,
-                                        [&](uint32_t id) {
-                                          if (k < d) dst[k] = id;
-                                          k++;
-                                        });
-      if (r != int64_t(d)) {
-        set_error(a.err, kErrBadStream);
-        for (uint32_t q = (r > 0 ? uint32_t(r) : 0u); q < d; q++) dst[q] = g.vertices[p];
+    const bool hub = sg.end - sg.begin == 1 && g.deg[sg.begin] > kV1MaxDeg;
+    if (!hub) {
+      const uint32_t nchunks = (sg.end - sg.begin + 31) / 32;
+      for (uint32_t ch = warp; ch < nchunks; ch += kWarps) {
+        const uint32_t p0 = sg.begin + ch * 32;
+        const uint32_t p = p0 + lane;
+        const bool valid = p < sg.end;
+        const uint32_t node = valid ? g.vertices[p] : 0u;
+        const uint32_t d = valid ? g.deg[p] : 0u;
+        const uint64_t o0 = a.arc_off[p0];
+        const uint32_t base = valid ? uint32_t(a.arc_off[p] - o0) : 0u;
+        if (!warp_decode_batch(g, a.scratch + o0, valid, p, node, d, base, lane) && lane == 0)
+          set_error(a.err, kErrBadStream);
       }
+    } else {
+      const uint32_t p = sg.begin;
+      const uint32_t node = g.vertices[p];
+      const uint32_t d = g.deg[p];
+      uint32_t *out = a.scratch + a.arc_off[p];
+      const uint64_t end = g.offsets[p + 1];
+      bool bad = false;
+      if (t == 0) {
+        BitReader r;
+        r.seek(g.words, g.offsets[p]);
+        uint32_t ns = r.segcnt(bad);
+        if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
+          bad = true;
+          ns = 0;
+        }
+        sh.nseg_i = ns;
+        sh.ibase = r.pos;
+        sh.last_end = r.pos;
+        sh.items = 0;
+        sh.bad = bad ? 1u : 0u;
+      }
+      __syncthreads();
+      const uint32_t nseg_i = sh.nseg_i;
+      uint32_t written = 0;  // block-uniform item cursor
+      for (uint32_t j0 = 0; j0 < nseg_i; j0 += kThreads) {
+        const uint32_t j = j0 + t;
+        bool has = j < nseg_i;
+        BitReader r;
+        uint32_t cnt = 0, cc = 0, left = 0;
+        const uint64_t q = sh.ibase + uint64_t(kSegBits) * j;
+        if (has) {
+          if (q >= end) {
+            bad = true;
+            has = false;
+          } else {
+            r.seek(g.words, q);
+            cnt = r.gamma(bad);
+          }
+        }
+        while (__syncthreads_or(has && cc < cnt)) {
+          uint32_t len = 0;
+          if (has && cc < cnt) {
+            const uint32_t l = r.gamma(bad);
+            left = (cc == 0) ? zigzag_first(node, l) : left + l + 1u;
+            len = r.gamma(bad) + kMinItv;
+            cc++;
+            if (bad || r.pos > end || uint64_t(left) + len > g.n) {
+              bad = true;
+              len = 0;
+              cnt = cc;
+            }
+          }
+          sh.left[t] = left;
+          const uint32_t total = block_scan(sh, len);
+          if (len) left += len;
+          for (uint32_t i0 = t; i0 < total; i0 += kThreads) {
+            uint32_t lo = 0, hi = kThreads - 1;
+            while (lo < hi) {
+              const uint32_t mid = (lo + hi + 1) >> 1;
+              if (sh.pref[mid] <= i0) lo = mid;
+              else hi = mid - 1;
+            }
+            if (written + i0 < d) out[written + i0] = sh.left[lo] + (i0 - sh.pref[lo]);
+          }
+          written += total;
+          __syncthreads();
+        }
+        if (has && j == nseg_i - 1) sh.last_end = r.pos;
+      }
+      __syncthreads();
+      if (t == 0) {
+        BitReader r;
+        r.seek(g.words, sh.last_end);
+        uint32_t ns = r.segcnt(bad);
+        if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
+          bad = true;
+          ns = 0;
+        }
+        sh.nseg_r = ns;
+        sh.rbase = r.pos;
+        sh.last_end = r.pos;
+      }
+      __syncthreads();
+      const uint32_t nseg_r = sh.nseg_r;
+      for (uint32_t j0 = 0; j0 < nseg_r; j0 += kThreads) {
+        const uint32_t j = j0 + t;
+        bool has = j < nseg_r;
+        BitReader r;
+        uint32_t cnt = 0;
+        if (has) {
+          const uint64_t q = sh.rbase + uint64_t(kSegBits) * j;
+          if (q >= end) {
+            bad = true;
+            has = false;
+          } else {
+            r.seek(g.words, q);
+            cnt = r.gamma(bad);
+            if (bad) cnt = 0;
+          }
+        }
+        const uint32_t total = block_scan(sh, cnt);
+        if (has) {
+          uint32_t o = written + sh.pref[t], v = 0;
+          for (uint32_t cc = 0; cc < cnt; cc++) {
+            const uint32_t x = r.zeta3(bad);
+            v = (cc == 0) ? zigzag_first(node, x) : v + x + 1u;
+            if (bad || r.pos > end || uint64_t(v) >= g.n || o >= d) {
+              bad = true;
+              break;
+            }
+            out[o++] = v;
+          }
+          if (j == nseg_r - 1) sh.last_end = r.pos;
+        }
+        written += total;
+        __syncthreads();
+      }
+      if (bad) sh.bad = 1;
+      __syncthreads();
+      if (sh.bad || sh.last_end != end || written != d) {
+        // keep every scratch id in range; the error word reports the stream
+        for (uint32_t k = t; k < d; k += kThreads) out[k] = node;
+        if (t == 0) set_error(a.err, kErrBadStream);
+      }
+      __syncthreads();
     }
-    if (a.seg_cycles && threadIdx.x == 0)
+    if (a.seg_cycles && t == 0)
       atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s),
                 (unsigned long long)((clock64() - t0) * kWarps));
+    __syncthreads();
   }
 }
 

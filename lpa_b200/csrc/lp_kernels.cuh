@@ -18,14 +18,13 @@ enum Variant : int {
 
 constexpr int kThreads = 256;             // threads per block of the iteration kernel
 constexpr int kWarps = kThreads / 32;
-constexpr uint32_t kStage = 8192;         // staged ids/labels per block
-constexpr uint32_t kTableSlots = 4096;    // exact-count slots per block
-constexpr uint32_t kWarpSlots = kTableSlots / kWarps;  // per warp in warp-counting mode
-constexpr uint32_t kV1MaxDeg = kWarpSlots / 2;         // 256
+constexpr uint32_t kStage = 8192;         // staged ids/labels per block (1024 per warp)
+constexpr uint32_t kTableSlots = 8192;    // exact-count slots per block (1024 per warp)
+constexpr uint32_t kWarpStage = kStage / kWarps;
+constexpr uint32_t kWarpSlots = kTableSlots / kWarps;
+constexpr uint32_t kV1MaxDeg = kWarpSlots - 1;         // 1023: a warp's table holds every distinct label
 constexpr uint32_t kV2MaxDeg = 32;
 constexpr uint32_t kBlockMaxSmemDeg = kTableSlots / 2; // exact degrees counted in shared memory
-constexpr uint32_t kTileMax = kThreads;   // positions per light tile (one per thread)
-constexpr uint32_t kResSegChunk = 128;    // residual segments staged per round (<= 64 items each)
 
 // dynamic shared memory of the iteration kernel
 constexpr size_t kSmemBytes = size_t(kStage) * 4 + size_t(kTableSlots) * 8;
