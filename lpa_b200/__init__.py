@@ -466,6 +466,49 @@ def mlp_predict(params, x, device=0):
     return out
 
 
+class Batch:
+    """Many graphs propagated together by one persistent launch (lpa_batch_*)."""
+
+    def __init__(self, graphs, **opts):
+        descs = [g.desc() if isinstance(g, HostGraph) else g for g in graphs]
+        arr = (GraphDesc * len(descs))()
+        for i, d in enumerate(descs):
+            C.memmove(C.byref(arr, i * C.sizeof(GraphDesc)), C.byref(d), C.sizeof(GraphDesc))
+        self._keep = (graphs, descs, arr)
+        self.n = [int(d.num_vertices) for d in descs]
+        o = default_opts(**opts)
+        out = C.c_void_p()
+        _check(lib().lpa_batch_create(arr, len(descs), C.byref(o), C.byref(out)), "lpa_batch_create")
+        self._h = out
+
+    def run(self, max_iter: int, early_exit: bool = True) -> np.ndarray:
+        iters = np.zeros(len(self.n), np.uint32)
+        _check(lib().lpa_batch_run(self._h, max_iter, int(early_exit), _ptr(iters, C.c_uint32)), "lpa_batch_run")
+        return iters
+
+    def labels(self, i: int) -> np.ndarray:
+        out = np.empty(self.n[i], np.uint32)
+        _check(lib().lpa_batch_get_labels(self._h, i, _ptr(out, C.c_uint32), self.n[i]), "lpa_batch_get_labels")
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lpa_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class LabelPropagator:
     """Mirror of the reference's propagator interface
     (include/label_propagator.h:11-38; baselines/novaplus/novaplus_propogator.cuh:100-129):

@@ -368,6 +368,50 @@ __device__ __forceinline__ void table_add(uint32_t *keys, uint32_t *cnts, uint32
   }
 }
 
+// Exact counter in shared memory without clearing: a slot is one 64-bit word
+// [epoch:16 | label:32 | count:16].  A slot whose epoch is not the current
+// one is empty, so a new vertex only bumps the epoch.  insert() returns the
+// label's count after the increment, so the caller keeps a running argmax and
+// never scans the table.  cap (a power of two) must exceed the number of
+// distinct labels inserted under one epoch; counts must stay below 65536.
+struct EpochTable {
+  unsigned long long *slots;
+  uint32_t cap;
+  uint32_t epoch;  // 1..65535
+  __device__ __forceinline__ uint32_t insert(uint32_t label, uint32_t c) const {
+    const unsigned long long tag = (uint64_t(epoch) << 48) | (uint64_t(label) << 16);
+    uint32_t h = slot_hash(label) & (cap - 1);
+    for (uint32_t probe = 0; probe < 2 * cap; probe++) {
+      const unsigned long long v = slots[h];
+      if (uint32_t(v >> 48) == epoch) {
+        if ((v & ~0xFFFFull) == tag) {
+          const unsigned long long old = atomicAdd(&slots[h], (unsigned long long)c);
+          return uint32_t(old & 0xFFFFull) + c;
+        }
+        h = (h + 1) & (cap - 1);
+        continue;
+      }
+      if (atomicCAS(&slots[h], v, tag | c) == v) return c;
+      // another lane claimed the slot first: look at it again
+    }
+    return 0;
+  }
+};
+
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Bulk prefetch of [p, p + bytes) into L2 (cp.async.bulk.prefetch, sm_90+):
+// one instruction per range, rounded out to 16-byte boundaries, split into
+// pieces below 1 MiB.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint64_t bytes) {
+  if (!p || bytes == 0) return;
+  uint64_t a = reinterpret_cast<uint64_t>(p) & ~uint64_t(15);
+  const uint64_t e = (reinterpret_cast<uint64_t>(p) + bytes + 15) & ~uint64_t(15);
+  while (a < e) {
+    const uint32_t n = uint32_t(e - a < (1u << 20) ? e - a : (1u << 20));
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(n) : "memory");
+    a += n;
+  }
+}
 
 }  // namespace lpa_dev

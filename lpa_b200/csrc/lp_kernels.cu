@@ -25,6 +25,12 @@ namespace lpa_dev {
 
 namespace {
 
+// Epoch ranges of the shared tables: warp tables use [1, kLightEpochs), the
+// block table [kLightEpochs, 65536), so a slot left by one mode never matches
+// the other.
+constexpr uint32_t kLightEpochs = 32768;
+constexpr uint32_t kHeavyEpochFirst = 32768;
+
 __device__ __forceinline__ uint32_t next_pow2(uint32_t x) { return x <= 1 ? 1u : (1u << (32 - __clz(x - 1))); }
 
 struct Ctx {
@@ -32,7 +38,14 @@ struct Ctx {
   uint32_t *lab_out;
   unsigned long long *changed;
   uint32_t it;
+  bool coherent;  // labels may change within the launch (batched graphs): read them through L2
 };
+
+// A label read: the non-coherent path when labels are fixed for the whole
+// launch, else an L2 (ld.global.cg) read.
+__device__ __forceinline__ uint32_t ld_label(const Ctx &c, uint32_t i) {
+  return c.coherent ? __ldcg(c.lab_in + i) : __ldg(c.lab_in + i);
+}
 
 __device__ __forceinline__ Ctx resolve(const IterArgs &a) {
   Ctx c;
@@ -41,6 +54,7 @@ __device__ __forceinline__ Ctx resolve(const IterArgs &a) {
   c.lab_in = par ? a.labs1 : a.labs0;
   c.lab_out = par ? a.labs0 : a.labs1;
   c.changed = a.changed + (a.it_dev ? c.it : 0u);
+  c.coherent = false;
   return c;
 }
 
@@ -66,6 +80,7 @@ struct BlockSh {
   uint64_t red[kWarps];
   uint64_t ibase, rbase, last_end;
   uint32_t nseg_i, nseg_r, item, items, bad;
+  uint32_t hepoch;  // epoch of the block's exact table
 };
 
 // Block-wide exclusive scan of v into sh.pref; returns the total.
@@ -90,11 +105,23 @@ __device__ __forceinline__ uint32_t block_scan(BlockSh &sh, uint32_t v) {
 // Called warp-synchronously by every lane; ok marks a real label.  Lanes of a
 // warp holding the same label are merged first (match.any), so each distinct
 // label of a step touches the table once.
-struct ExactSink {
+struct ExactSink {  // global table (key/count arrays, cleared after use)
   uint32_t *keys, *cnts, cap;
   __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
     const uint32_t m = __match_any_sync(kFull, ok ? lab : kFull);
     if (ok && (__ffs(m) - 1) == int(threadIdx.x & 31u)) table_add(keys, cnts, cap, lab, __popc(m));
+  }
+};
+
+struct EpochSink {  // shared epoch table with a running argmax per thread
+  EpochTable et;
+  uint64_t *best;
+  __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
+    const uint32_t m = __match_any_sync(kFull, ok ? lab : kFull);
+    if (ok && (__ffs(m) - 1) == int(threadIdx.x & 31u)) {
+      const uint64_t cand = pack_best(et.insert(lab, __popc(m)), lab);
+      if (cand > *best) *best = cand;
+    }
   }
 };
 
@@ -133,13 +160,13 @@ struct CmsBestSink {
 
 // Labels of the global ids src[0..total) into stage.
 __device__ __forceinline__ void block_gather_from(uint32_t *stage, const uint32_t *__restrict__ src, uint32_t total,
-                                                  const uint32_t *__restrict__ lab_in) {
+                                                  const Ctx &c) {
   for (uint32_t k0 = threadIdx.x; k0 < total; k0 += 4 * kThreads) {
     uint32_t v[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const uint32_t k = k0 + u * kThreads;
-      v[u] = k < total ? __ldg(lab_in + __ldg(src + k)) : 0u;
+      v[u] = k < total ? ld_label(c, __ldg(src + k)) : 0u;
     }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
@@ -171,7 +198,7 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
     const uint32_t *src = (p >= g.n_c) ? g.small_nbr + g.small_off[p - g.n_c] : a.scratch + a.arc_off[p];
     for (uint32_t c0 = 0; c0 < d; c0 += kStage) {
       const uint32_t cnt = min(kStage, d - c0);
-      block_gather_from(stage, src + c0, cnt, c.lab_in);
+      block_gather_from(stage, src + c0, cnt, c);
       __syncthreads();
       block_consume_stage(stage, cnt, sink);
       __syncthreads();
@@ -245,7 +272,7 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
               if (sh.pref[mid] <= i) lo = mid;
               else hi = mid - 1;
             }
-            lab[u] = __ldg(c.lab_in + sh.left[lo] + (i - sh.pref[lo]));
+            lab[u] = ld_label(c, sh.left[lo] + (i - sh.pref[lo]));
             my_items++;
           }
         }
@@ -327,7 +354,7 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           const uint32_t k = k0 + 32 * u;
-          lv[u] = k < total ? __ldg(c.lab_in + wst[k]) : 0u;
+          lv[u] = k < total ? ld_label(c, wst[k]) : 0u;
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {
@@ -377,7 +404,7 @@ __device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint3
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   const uint32_t node = g.vertices[p];
   const uint32_t d = g.deg[p];
-  const uint32_t old = __ldg(c.lab_in + node);
+  const uint32_t old = ld_label(c, node);
   if (d == 0) return;
   uint64_t best = 0;
   if (a.cms_thr != 0 && d >= a.cms_thr) {
@@ -390,20 +417,29 @@ __device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint3
     else heavy_produce(a, c, sh, stage, p, node, d, from_scratch, s2);
     __syncthreads();
     for (uint32_t i = t; i < kCmsDepth * kCmsWidth; i += kThreads) cms[i] = 0u;
-  } else {
-    uint32_t *keys, *cnts;
-    const uint32_t cap = next_pow2(2 * d);
-    if (d <= kBlockMaxSmemDeg) {
-      keys = tab;
-      cnts = tab + kTableSlots;
-    } else {
-      if (a.gtab_slots == 0 || cap > a.gtab_slots) {
-        if (t == 0) set_error(a.err, kErrCapacity);
-        return;
-      }
-      keys = a.gtab + uint64_t(blockIdx.x) * 2 * a.gtab_slots;
-      cnts = keys + a.gtab_slots;
+  } else if (d <= kBlockMaxSmemDeg) {
+    unsigned long long *slots = reinterpret_cast<unsigned long long *>(tab);
+    if (t == 0) {
+      if (++sh.hepoch >= 65536u) sh.hepoch = 0;
     }
+    __syncthreads();
+    if (sh.hepoch == 0) {  // epochs used up: start the block table over
+      for (uint32_t i = t; i < kTableSlots; i += kThreads) slots[i] = 0ull;
+      __syncthreads();
+      if (t == 0) sh.hepoch = kHeavyEpochFirst;
+      __syncthreads();
+    }
+    const EpochTable et{slots, next_pow2(2 * d), sh.hepoch};
+    heavy_produce(a, c, sh, stage, p, node, d, from_scratch, EpochSink{et, &best});
+    __syncthreads();
+  } else {
+    const uint32_t cap = next_pow2(2 * d);
+    if (a.gtab_slots == 0 || cap > a.gtab_slots) {
+      if (t == 0) set_error(a.err, kErrCapacity);
+      return;
+    }
+    uint32_t *keys = a.gtab + uint64_t(blockIdx.x) * 2 * a.gtab_slots;
+    uint32_t *cnts = keys + a.gtab_slots;
     heavy_produce(a, c, sh, stage, p, node, d, from_scratch, ExactSink{keys, cnts, cap});
     __syncthreads();
     for (uint32_t i = t; i < cap; i += kThreads) {
@@ -568,8 +604,9 @@ __device__ bool warp_decode_batch(const DevGraph &g, uint32_t *stage, bool activ
 }
 
 // Up to 32 consecutive positions [p0, p1) by one warp.
-__device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, uint32_t *keys, uint32_t *cnts,
-                            uint32_t seg, uint32_t p0, uint32_t p1, int variant, unsigned long long &changed) {
+__device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, unsigned long long *slots,
+                            uint32_t &epoch, uint32_t seg, uint32_t p0, uint32_t p1, int variant,
+                            unsigned long long &changed) {
   const DevGraph &g = a.g;
   const uint32_t lane = threadIdx.x & 31u;
   constexpr uint32_t cap_stage = kWarpStage;
@@ -577,7 +614,7 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, ui
   const bool valid = p < p1;
   const uint32_t node = valid ? g.vertices[p] : 0u;
   uint32_t d = valid ? g.deg[p] : 0u;
-  const uint32_t old = valid ? __ldg(c.lab_in + node) : 0u;
+  const uint32_t old = valid ? ld_label(c, node) : 0u;
   const bool cgr = p0 < g.n_c;  // chunks never straddle the compressed / small boundary
   const bool decode = cgr && variant != kVarTwoPass;
   if (d > cap_stage || (variant == kVarPacked && d > kV2MaxDeg) || d > kV1MaxDeg) {
@@ -604,15 +641,15 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, ui
       set_error(a.err, kErrBadStream);
     __syncwarp();
     // 2. labels: every load of the batch in flight together
-    for (uint32_t k0 = lane; k0 < total; k0 += 128) {
-      uint32_t v[4];
+    for (uint32_t k0 = lane; k0 < total; k0 += 256) {
+      uint32_t v[8];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
+      for (int u = 0; u < 8; u++) {
         const uint32_t k = k0 + 32 * u;
-        v[u] = k < total ? __ldg(c.lab_in + (decode ? stage[k] : __ldg(src + src_skip + k))) : 0u;
+        v[u] = k < total ? ld_label(c, decode ? stage[k] : __ldg(src + src_skip + k)) : 0u;
       }
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
+      for (int u = 0; u < 8; u++) {
         const uint32_t k = k0 + 32 * u;
         if (k < total) stage[k] = v[u];
       }
@@ -662,23 +699,22 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, ui
           const uint32_t maxc = __reduce_max_sync(kFull, cnt);
           bestl = __reduce_min_sync(kFull, (ok && cnt == maxc) ? lab : kFull);
         } else {
-          const uint32_t cap = min(next_pow2(2 * dv), kWarpSlots);  // > dv: every label fits
+          // epoch table: no clearing, running argmax from the returned counts
+          if (++epoch >= kLightEpochs) {
+            for (uint32_t i = lane; i < kWarpSlots; i += 32) slots[i] = 0ull;
+            __syncwarp();
+            epoch = 1;
+          }
+          const EpochTable et{slots, min(next_pow2(2 * dv), kWarpSlots), epoch};  // cap > dv: every label fits
+          uint64_t bp = 0;
           for (uint32_t k0 = 0; k0 < dv; k0 += 32) {
             const uint32_t k = k0 + lane;
             const bool ok = k < dv;
             const uint32_t lab = ok ? stage[bv + k] : kFull;
             const uint32_t m = __match_any_sync(kFull, lab);
-            if (ok && (__ffs(m) - 1) == int(lane)) table_add(keys, cnts, cap, lab, __popc(m));
-          }
-          __syncwarp();
-          uint64_t bp = 0;
-          for (uint32_t i = lane; i < cap; i += 32) {
-            const uint32_t kk = keys[i];
-            if (kk) {
-              const uint64_t cand = pack_best(cnts[i], kk - 1u);
+            if (ok && (__ffs(m) - 1) == int(lane)) {
+              const uint64_t cand = pack_best(et.insert(lab, __popc(m)), lab);
               bp = cand > bp ? cand : bp;
-              keys[i] = 0u;
-              cnts[i] = 0u;
             }
           }
           bestl = best_label(warp_max_u64(bp));
@@ -711,19 +747,33 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
   uint32_t *tab = smem + kStage;  // kTableSlots keys + kTableSlots counts (or the sketch)
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   for (uint32_t i = t; i < 2 * kTableSlots; i += kThreads) tab[i] = 0u;
+  if (t == 0) sh.hepoch = kHeavyEpochFirst;
   __syncthreads();
   const Ctx c = resolve(a);
   unsigned long long changed = 0;
   uint32_t *qctr = a.work + 2 * (a.it_dev ? c.it : 0u);
 
-  // heavy items: one segment per block (largest first)
+  // heavy items: one segment per block (largest first).  The next item is
+  // claimed before the current one runs and its bits are prefetched into L2.
+  if (t == 0) {
+    const uint32_t i0 = atomicAdd(qctr, 1u);
+    sh.item = i0;
+    if (i0 < a.n_heavy) prefetch_l2(reinterpret_cast<const void *>(a.heavy[i0].pf_addr), a.heavy[i0].pf_bytes);
+  }
+  __syncthreads();
+  uint32_t next = sh.item;
   for (;;) {
-    if (t == 0) sh.item = atomicAdd(qctr, 1u);
-    __syncthreads();
-    const uint32_t i = sh.item;
+    const uint32_t i = next;
     __syncthreads();
     if (i >= a.n_heavy) break;
-    const uint32_t s = a.heavy[i];
+    if (t == 0) {
+      const uint32_t in = atomicAdd(qctr, 1u);
+      sh.item = in;
+      if (in < a.n_heavy) prefetch_l2(reinterpret_cast<const void *>(a.heavy[in].pf_addr), a.heavy[in].pf_bytes);
+    }
+    __syncthreads();
+    next = sh.item;
+    const uint32_t s = a.heavy[i].tag;
     const bool from_scratch = a.seg_var[s] == kVarTwoPass;
     const Seg sg = a.segs[s];
     const long long t0 = clock64();
@@ -733,25 +783,158 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
                 (unsigned long long)((clock64() - t0) * kWarps));
   }
 
-  // light chunks: one warp per chunk of up to 32 positions
-  uint32_t *wkeys = tab + warp * kWarpSlots;
-  uint32_t *wcnts = tab + kTableSlots + warp * kWarpSlots;
+  // light chunks: a warp claims 4 consecutive chunks at a time, prefetches
+  // the last 3 into L2 at once and runs them in order
+  unsigned long long *wslots = reinterpret_cast<unsigned long long *>(tab) + warp * kWarpSlots;
   uint32_t *wstage = stage + warp * kWarpStage;
+  uint32_t wepoch = 0;
   for (;;) {
-    uint32_t i = 0;
-    if (lane == 0) i = atomicAdd(qctr + 1, 1u);
-    i = __shfl_sync(kFull, i, 0);
-    if (i >= a.n_light) break;
-    const uint32_t item = a.light[i];
-    const uint32_t s = item >> 3;
-    const Seg sg = a.segs[s];
-    const uint32_t p0 = sg.begin + (item & 7u) * 32u;
-    const long long t0 = clock64();
-    light_chunk(a, c, wstage, wkeys, wcnts, s, p0, min(sg.end, p0 + 32u), a.seg_var[s], changed);
-    if (a.seg_cycles && lane == 0)
-      atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s), (unsigned long long)(clock64() - t0));
+    uint32_t i0 = 0;
+    if (lane == 0) i0 = atomicAdd(qctr + 1, 4u);
+    i0 = __shfl_sync(kFull, i0, 0);
+    if (i0 >= a.n_light) break;
+    WorkItem wi{};
+    if (lane < 4 && i0 + lane < a.n_light) wi = a.light[i0 + lane];
+    if (lane >= 1 && lane < 4 && i0 + lane < a.n_light)
+      prefetch_l2(reinterpret_cast<const void *>(wi.pf_addr), wi.pf_bytes);
+    for (uint32_t k = 0; k < 4 && i0 + k < a.n_light; k++) {
+      const uint32_t item = __shfl_sync(kFull, wi.tag, k);
+      const uint32_t s = item >> 3;
+      const Seg sg = a.segs[s];
+      const uint32_t p0 = sg.begin + (item & 7u) * 32u;
+      const long long t0 = clock64();
+      light_chunk(a, c, wstage, wslots, wepoch, s, p0, min(sg.end, p0 + 32u), a.seg_var[s], changed);
+      if (a.seg_cycles && lane == 0)
+        atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s), (unsigned long long)(clock64() - t0));
+    }
   }
   flush_changed(c.changed, changed);
+}
+
+// Many graphs, one persistent launch.  A ring queue holds (graph,
+// iteration, segment) items; iteration 0 of every graph is queued by the
+// host.  The block that finishes the last item of a graph's iteration reads
+// that iteration's changed count and either retires the graph or queues all
+// its segments for the next iteration, so an item never waits on another
+// item.  Blocks wait (bounded) only on an empty queue slot.  Labels change
+// during the launch, so they are read through L2.
+__global__ void __launch_bounds__(kThreads, 2) k_batch(BatchArgs b) {
+  extern __shared__ uint32_t smem[];
+  __shared__ BlockSh sh;
+  __shared__ IterArgs ia;
+  __shared__ unsigned long long s_item, s_enq_base;
+  __shared__ uint32_t s_last, s_enq;
+  uint32_t *stage = smem;
+  uint32_t *tab = smem + kStage;
+  const uint32_t t = threadIdx.x, warp = t >> 5;
+  for (uint32_t i = t; i < 2 * kTableSlots; i += kThreads) tab[i] = 0u;
+  if (t == 0) sh.hepoch = kHeavyEpochFirst;
+  __syncthreads();
+  unsigned long long *wslots = reinterpret_cast<unsigned long long *>(tab) + warp * kWarpSlots;
+  uint32_t *wstage = stage + warp * kWarpStage;
+  uint32_t wepoch = 0;
+  for (;;) {
+    if (t == 0) {
+      const unsigned long long idx = atomicAdd(b.head, 1ull);
+      volatile unsigned long long *slot = b.queue + (idx % b.cap);
+      unsigned long long e = *slot;
+      unsigned long long spins = 0;
+      while (e == kQueueEmpty) {
+        if (*reinterpret_cast<volatile uint32_t *>(b.active) == 0u) break;
+        if (++spins > b.spin_limit) {
+          set_error(b.err, kErrTimeout);
+          break;
+        }
+        __nanosleep(200);
+        e = *slot;
+      }
+      if (e != kQueueEmpty) *slot = kQueueEmpty;
+      __threadfence();
+      s_item = e;
+    }
+    __syncthreads();
+    const unsigned long long e = s_item;
+    if (e == kQueueEmpty) break;
+    const uint32_t gi = uint32_t(e >> 44), it = uint32_t(e >> 32) & 0xFFFu, s = uint32_t(e);
+    if (t == 0) {
+      const BatchGraph &bg = b.graphs[gi];
+      ia.g = bg.g;
+      ia.labs0 = bg.labs0;
+      ia.labs1 = bg.labs1;
+      ia.parity0 = 0;
+      ia.it_dev = nullptr;
+      ia.changed = b.changed + gi;
+      ia.work = nullptr;
+      ia.err = b.err;
+      ia.segs = bg.segs;
+      ia.seg_var = bg.seg_var;
+      ia.seg_cycles = nullptr;
+      ia.seg_changed = nullptr;
+      ia.cms_thr = b.cms_thr;
+      for (int r = 0; r < kCmsDepth; r++) ia.seeds[r] = b.seeds[r];
+      ia.scratch = nullptr;
+      ia.arc_off = nullptr;
+      ia.gtab = b.gtab;
+      ia.gtab_slots = b.gtab_slots;
+    }
+    __syncthreads();
+    Ctx c;
+    c.it = it;
+    c.lab_in = (it & 1u) ? ia.labs1 : ia.labs0;
+    c.lab_out = (it & 1u) ? ia.labs0 : ia.labs1;
+    c.changed = ia.changed;
+    c.coherent = true;
+    unsigned long long changed = 0;
+    const Seg sg = ia.segs[s];
+    const int v = ia.seg_var[s];
+    if (v == kVarBlock || v == kVarTwoPass) {
+      for (uint32_t p = sg.begin; p < sg.end; p++) heavy_vertex(ia, c, sh, stage, tab, s, p, false, changed);
+    } else {
+      const uint32_t p0 = sg.begin + warp * 32u;  // light segments hold at most 8 chunks
+      if (p0 < sg.end) light_chunk(ia, c, wstage, wslots, wepoch, s, p0, min(sg.end, p0 + 32u), v, changed);
+    }
+    flush_changed(c.changed, changed);
+    __threadfence();
+    __syncthreads();
+    if (t == 0) {
+      const uint32_t nseg = b.graphs[gi].nseg;
+      s_last = (atomicAdd(b.done_items + gi, 1u) + 1u == nseg) ? 1u : 0u;
+      s_enq = 0;
+      if (s_last) {
+        __threadfence();
+        const unsigned long long ch = atomicExch(b.changed + gi, 0ull);
+        b.done_items[gi] = 0;
+        b.iters[gi] = it + 1;
+        const bool stop = (b.early_exit && ch == 0ull) || it + 1 >= b.max_iter;
+        if (stop) {
+          __threadfence();
+          atomicSub(b.active, 1u);
+        } else {
+          s_enq_base = atomicAdd(b.tail, (unsigned long long)nseg);
+          s_enq = nseg;
+        }
+      }
+    }
+    __syncthreads();
+    if (s_enq) {
+      const unsigned long long tag = (uint64_t(gi) << 44) | (uint64_t(it + 1) << 32);
+      for (uint32_t k = t; k < s_enq; k += kThreads) {
+        __threadfence();
+        b.queue[(s_enq_base + k) % b.cap] = tag | k;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs) {
+  for (uint32_t gi = blockIdx.x; gi < ngraphs; gi += gridDim.x) {
+    const BatchGraph &bg = graphs[gi];
+    for (uint64_t v = threadIdx.x; v < bg.g.n; v += blockDim.x) {
+      bg.labs0[v] = uint32_t(v);
+      bg.labs1[v] = uint32_t(v);
+    }
+  }
 }
 
 // Two-pass variant, pass 1: the two-pass segments' compressed positions are

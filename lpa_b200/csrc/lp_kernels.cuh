@@ -19,18 +19,26 @@ enum Variant : int {
 constexpr int kThreads = 256;             // threads per block of the iteration kernel
 constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kStage = 8192;         // staged ids/labels per block (1024 per warp)
-constexpr uint32_t kTableSlots = 8192;    // exact-count slots per block (1024 per warp)
+constexpr uint32_t kTableSlots = 8192;    // 64-bit exact-count slots per block (1024 per warp)
 constexpr uint32_t kWarpStage = kStage / kWarps;
 constexpr uint32_t kWarpSlots = kTableSlots / kWarps;
 constexpr uint32_t kV1MaxDeg = kWarpSlots - 1;         // 1023: a warp's table holds every distinct label
 constexpr uint32_t kV2MaxDeg = 32;
-constexpr uint32_t kBlockMaxSmemDeg = kTableSlots / 2; // exact degrees counted in shared memory
+constexpr uint32_t kBlockMaxSmemDeg = kTableSlots / 2; // exact degrees counted in shared memory (<= 4095)
 
 // dynamic shared memory of the iteration kernel
 constexpr size_t kSmemBytes = size_t(kStage) * 4 + size_t(kTableSlots) * 8;
 
 struct Seg {
   uint32_t begin, end;  // positions [begin, end)
+};
+
+// A work item with the device range it will read, so a warp or block can
+// prefetch items it has claimed but not started.
+struct WorkItem {
+  uint32_t tag;        // heavy: segment id; light: (segment << 3) | 32-position chunk
+  uint32_t pf_bytes;   // bytes of the range to prefetch
+  uint64_t pf_addr;    // device address of the range (bitstream bits, small-CSR ids or scratch ids)
 };
 
 struct IterArgs {
@@ -43,9 +51,9 @@ struct IterArgs {
   uint32_t *err;
   const Seg *segs;              // all segments
   const uint8_t *seg_var;       // variant per segment
-  const uint32_t *heavy;        // block work items: segment ids, largest first
+  const WorkItem *heavy;        // block work items (one segment each), largest first
   uint32_t n_heavy;
-  const uint32_t *light;        // warp work items: (segment << 3) | 32-position chunk
+  const WorkItem *light;        // warp work items (32-position chunks)
   uint32_t n_light;
   const uint32_t *two_pass;     // segments decoded by the two-pass pre-pass
   uint32_t n_two_pass;
@@ -62,6 +70,41 @@ struct IterArgs {
 };
 
 __device__ __forceinline__ uint32_t iter_index(const IterArgs &a) { return a.it_dev ? *a.it_dev : 0u; }
+
+// ---- many graphs in one persistent launch ------------------------------
+struct BatchGraph {
+  DevGraph g;
+  uint32_t *labs0, *labs1;
+  const Seg *segs;
+  const uint8_t *seg_var;
+  uint32_t nseg;
+};
+
+// Queue items: (graph << 44) | (iteration << 32) | segment.
+constexpr unsigned long long kQueueEmpty = ~0ull;
+
+struct BatchArgs {
+  const BatchGraph *graphs;
+  uint32_t ngraphs;
+  unsigned long long *queue;      // ring of items
+  uint32_t cap;                   // ring capacity (> items of one iteration of every graph)
+  unsigned long long *head, *tail;
+  uint32_t *active;               // graphs still running
+  uint32_t *done_items;           // per graph: items finished in its current iteration
+  unsigned long long *changed;    // per graph: changed count of its current iteration
+  uint32_t *iters;                // per graph: iterations finished
+  uint32_t *err;
+  uint32_t max_iter;
+  int early_exit;
+  uint32_t cms_thr;
+  uint32_t seeds[kCmsDepth];
+  uint32_t *gtab;
+  uint32_t gtab_slots;
+  unsigned long long spin_limit;  // bound on the wait for an empty queue
+};
+
+__global__ void k_batch(BatchArgs b);
+__global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs);
 
 __global__ void k_iterate(IterArgs a);
 __global__ void k_decode_two_pass(IterArgs a);

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "lp_kernels.cuh"
@@ -139,9 +140,8 @@ int fixed_variant(const SegInfo &s) {
 }  // namespace lpa_rt
 
 // ------------------------------------------------------------------ plan ---
-static void build_segments(lpa_handle *h) {
-  h->segs.clear();
-  const uint32_t cms = h->opts.cms_threshold;
+std::vector<SegInfo> lpa_rt::make_segments(const uint32_t *deg, uint64_t n, uint64_t n_c, uint32_t cms) {
+  std::vector<SegInfo> segs;
   auto bucket_of = [&](uint32_t d) -> uint8_t {
     if ((cms != 0 && d >= cms) || d > kV1MaxDeg) return kHeavy;
     if (d < 16) return kTiny;
@@ -151,12 +151,12 @@ static void build_segments(lpa_handle *h) {
   SegInfo cur{};
   bool open = false;
   auto close = [&]() {
-    if (open) h->segs.push_back(cur);
+    if (open) segs.push_back(cur);
     open = false;
   };
-  for (uint64_t p = 0; p < h->n; p++) {
-    const uint32_t d = h->h_deg[p];
-    const uint8_t region = p < h->n_c ? 0 : 1;
+  for (uint64_t p = 0; p < n; p++) {
+    const uint32_t d = deg[p];
+    const uint8_t region = p < n_c ? 0 : 1;
     if (d == 0) {
       // isolated vertices need no work; they only end a segment
       close();
@@ -176,46 +176,82 @@ static void build_segments(lpa_handle *h) {
     cur.arcs += d;
   }
   close();
+  return segs;
+}
+
+static void build_segments(lpa_handle *h) {
+  h->segs = make_segments(h->h_deg.data(), h->n, h->n_c, h->opts.cms_threshold);
+}
+
+// The device range a work item over positions [p0, p1) will read.
+static WorkItem make_item(const lpa_handle *h, uint32_t tag, uint32_t p0, uint32_t p1, bool two_pass) {
+  WorkItem w{tag, 0, 0};
+  uint64_t addr = 0, bytes = 0;
+  if (p0 < h->n_c) {
+    if (two_pass) {
+      addr = reinterpret_cast<uint64_t>(h->d_scratch + h->h_arc_off[p0]);
+      bytes = (h->h_arc_off[p1] - h->h_arc_off[p0]) * 4;
+    } else {
+      const uint64_t b = h->h_offsets[p0] >> 5, e = h->h_offsets[p1] >> 5;
+      addr = reinterpret_cast<uint64_t>(h->d_words + b);
+      bytes = (e - b + 3) * 4;
+    }
+  } else {
+    const uint64_t b = h->h_small_off[p0 - h->n_c], e = h->h_small_off[p1 - h->n_c];
+    addr = reinterpret_cast<uint64_t>(h->d_small_nbr + b);
+    bytes = (e - b) * 4;
+  }
+  w.pf_addr = addr;
+  w.pf_bytes = uint32_t(std::min<uint64_t>(bytes, 0x7FFFFFFFull));
+  return w;
 }
 
 static void upload_lists(lpa_handle *h) {
   // heavy items: segments counted by a whole block (largest first); light
   // items: 32-position chunks of the others; two-pass segments of the
   // compressed region are decoded by the pre-pass.
-  std::vector<uint32_t> heavy, light, two;
+  std::vector<WorkItem> heavy, light;
+  std::vector<uint32_t> two;
   for (size_t s = 0; s < h->segs.size(); s++) {
     const int v = h->variant[s];
     const SegInfo &si = h->segs[s];
-    const bool block = v == LPA_VARIANT_BLOCK ||
-                       (v == LPA_VARIANT_TWO_PASS && !variant_capable(LPA_VARIANT_WARP, si, h->opts.cms_threshold));
+    const bool tp = v == LPA_VARIANT_TWO_PASS;
+    const bool block = v == LPA_VARIANT_BLOCK || (tp && !variant_capable(LPA_VARIANT_WARP, si, h->opts.cms_threshold));
     if (block) {
-      heavy.push_back(uint32_t(s));
+      heavy.push_back(make_item(h, uint32_t(s), si.begin, si.end, tp));
     } else {
       const uint32_t chunks = (si.end - si.begin + 31) / 32;
-      for (uint32_t c = 0; c < chunks; c++) light.push_back((uint32_t(s) << 3) | c);
+      for (uint32_t c = 0; c < chunks; c++) {
+        const uint32_t p0 = si.begin + 32 * c, p1 = std::min(si.end, p0 + 32);
+        light.push_back(make_item(h, (uint32_t(s) << 3) | c, p0, p1, tp));
+      }
     }
-    if (v == LPA_VARIANT_TWO_PASS && si.region == 0) two.push_back(uint32_t(s));
+    if (tp && si.region == 0) two.push_back(uint32_t(s));
   }
-  std::stable_sort(heavy.begin(), heavy.end(),
-                   [&](uint32_t a, uint32_t b) { return h->segs[a].arcs > h->segs[b].arcs; });
+  std::stable_sort(heavy.begin(), heavy.end(), [&](const WorkItem &a, const WorkItem &b) {
+    return h->segs[a.tag].arcs > h->segs[b.tag].arcs;
+  });
   h->n_heavy = uint32_t(heavy.size());
   h->n_light = uint32_t(light.size());
   h->n_two_pass = uint32_t(two.size());
-  std::vector<uint32_t> all;
-  all.reserve(heavy.size() + light.size() + two.size());
+  std::vector<WorkItem> all;
+  all.reserve(heavy.size() + light.size());
   all.insert(all.end(), heavy.begin(), heavy.end());
   all.insert(all.end(), light.begin(), light.end());
-  all.insert(all.end(), two.begin(), two.end());
-  if (all.size() > h->lists_cap) {
-    if (h->d_lists) {
-      auto it = std::find(h->allocations.begin(), h->allocations.end(), (void *)h->d_lists);
+  auto regrow = [&](auto *&ptr, size_t &cap, size_t need, const char *what) {
+    if (need <= cap && ptr) return;
+    if (ptr) {
+      auto it = std::find(h->allocations.begin(), h->allocations.end(), (void *)ptr);
       if (it != h->allocations.end()) h->allocations.erase(it);
-      cudaFree(h->d_lists);
+      cudaFree(ptr);
     }
-    h->lists_cap = all.size() + all.size() / 4 + 16;
-    h->d_lists = dalloc<uint32_t>(h, h->lists_cap, "work lists");
-  }
-  h2d(h, h->d_lists, all.data(), all.size(), "upload work lists");
+    cap = need + need / 4 + 16;
+    ptr = dalloc<std::remove_reference_t<decltype(*ptr)>>(h, cap, what);
+  };
+  regrow(h->d_items, h->items_cap, all.size(), "work items");
+  regrow(h->d_two, h->two_cap, two.size(), "two-pass list");
+  h2d(h, h->d_items, all.data(), all.size(), "upload work items");
+  h2d(h, h->d_two, two.data(), two.size(), "upload two-pass list");
   h2d(h, h->d_seg_var, h->variant.data(), h->variant.size(), "upload variants");
   check(h, cudaStreamSynchronize(h->stream), "upload work lists");
   h->plan_version++;
@@ -224,7 +260,8 @@ static void upload_lists(lpa_handle *h) {
 
 static void ensure_two_pass_scratch(lpa_handle *h) {
   if (h->d_scratch) return;
-  std::vector<uint64_t> off(h->n + 1, 0);
+  std::vector<uint64_t> &off = h->h_arc_off;
+  off.assign(h->n + 1, 0);
   for (uint64_t p = 0; p < h->n; p++) off[p + 1] = off[p] + h->h_deg[p];
   h->d_arc_off = dalloc<uint64_t>(h, h->n + 1, "arc offsets");
   h2d(h, h->d_arc_off, off.data(), h->n + 1, "upload arc offsets");
@@ -326,11 +363,11 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.err = h->d_err;
   a.segs = h->d_segs;
   a.seg_var = h->d_seg_var;
-  a.heavy = h->d_lists;
+  a.heavy = h->d_items;
   a.n_heavy = h->n_heavy;
-  a.light = h->d_lists + h->n_heavy;
+  a.light = h->d_items + h->n_heavy;
   a.n_light = h->n_light;
-  a.two_pass = h->d_lists + h->n_heavy + h->n_light;
+  a.two_pass = h->d_two;
   a.n_two_pass = h->n_two_pass;
   a.seg_cycles = (h->opts.record_timings >= 2 || h->collect_cycles) ? h->d_seg_cycles : nullptr;
   a.seg_changed = h->learner ? h->d_seg_changed : nullptr;
@@ -494,6 +531,9 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     for (auto &e : h->ev) check(h, cudaEventCreate(&e), "events");
     h->events_ready = true;
 
+    h->h_offsets.assign(g->offsets, g->offsets + (n_c ? n_c + 1 : 0));
+    if (n_c == 0) h->h_offsets.assign(1, 0);
+    if (n > n_c) h->h_small_off.assign(g->small_offset, g->small_offset + (n - n_c + 1));
     build_plan(h);
     // per-segment stream bits for the cost model's features
     for (auto &s : h->segs)

@@ -40,6 +40,8 @@ inline uint32_t next_pow2_host(uint64_t x) {
 
 bool variant_capable(int variant, const SegInfo &s, uint32_t cms_thr);
 int fixed_variant(const SegInfo &s);
+// Segments of a graph from its degrees by position (runs of one bucket).
+std::vector<SegInfo> make_segments(const uint32_t *deg, uint64_t n, uint64_t n_c, uint32_t cms_thr);
 
 }  // namespace lpa_rt
 
@@ -72,9 +74,13 @@ struct lpa_handle {
   std::vector<uint8_t> fixed;    // per segment, the heuristic's choice
   lpa_dev::Seg *d_segs = nullptr;
   uint8_t *d_seg_var = nullptr;
-  uint32_t *d_lists = nullptr;  // heavy items | light chunk items | two-pass segments
+  lpa_dev::WorkItem *d_items = nullptr;  // heavy items | light chunk items
+  uint32_t *d_two = nullptr;              // two-pass segments
   uint32_t n_heavy = 0, n_light = 0, n_two_pass = 0;
-  size_t lists_cap = 0;
+  size_t items_cap = 0, two_cap = 0;
+  std::vector<uint64_t> h_offsets;        // host copies for the prefetch ranges
+  std::vector<uint32_t> h_small_off;
+  std::vector<uint64_t> h_arc_off;
   int grid = 0;          // persistent iteration kernel
   int grid_decode = 0;   // two-pass decode kernel
   int occ = 1;
