@@ -408,7 +408,11 @@ __device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint3
   if (d == 0) return;
   uint64_t best = 0;
   if (a.cms_thr != 0 && d >= a.cms_thr) {
-    uint32_t *cms = tab;  // zero on entry
+    // the sketch shares its memory with the exact tables, whose slots are
+    // never cleared: zero the counters first
+    uint32_t *cms = tab;
+    for (uint32_t i = t; i < kCmsDepth * kCmsWidth; i += kThreads) cms[i] = 0u;
+    __syncthreads();
     const bool staged = heavy_produce(a, c, sh, stage, p, node, d, from_scratch, CmsAddSink{cms, a.seeds});
     __syncthreads();
     CmsBestSink s2{cms, a.seeds, &best};
@@ -416,6 +420,7 @@ __device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint3
     else if ((p >= g.n_c || from_scratch) && d <= kStage) block_consume_stage(stage, d, s2);
     else heavy_produce(a, c, sh, stage, p, node, d, from_scratch, s2);
     __syncthreads();
+    // leave no counter behind that an epoch table could read as its own slot
     for (uint32_t i = t; i < kCmsDepth * kCmsWidth; i += kThreads) cms[i] = 0u;
   } else if (d <= kBlockMaxSmemDeg) {
     unsigned long long *slots = reinterpret_cast<unsigned long long *>(tab);
