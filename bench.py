@@ -44,6 +44,13 @@ WORKLOADS = {
     # smaller R-MAT for quick checks
     "rmat-s20": dict(kind="rmat", scale=20, edge_factor=16.0, seed=1, small_thresh=32, cms=1024, iters=20),
     "rmat-s22": dict(kind="rmat", scale=22, edge_factor=16.0, seed=1, small_thresh=32, cms=1024, iters=20),
+    # web-like copy model: 100M vertices, out-degree 30 (prototype copies p=0.6 with
+    # offsets in [-8,8], else Zipf(1.1) targets); threshold 16, sketch >= 4096
+    "copy-100m": dict(kind="copy", n=100_000_000, out_degree=30, seed=1, small_thresh=16, cms=4096, iters=10),
+    # many uneven graphs in one persistent launch: vertex counts log-uniform in
+    # [1k, 256k], even graphs road grids (p=0.7), odd graphs R-MAT (edge factor 8),
+    # threshold 16, per-graph early exit (the 4096-graph [1k, 2M] batch scaled down)
+    "batch-256": dict(kind="batch", graphs=256, n_lo=1000, n_hi=262144, seed=1, small_thresh=16, cms=0, iters=30),
 }
 
 
@@ -81,10 +88,108 @@ def build_graph(w: dict):
 
     if w["kind"] == "rmat":
         g = L.HostGraph.rmat(w["scale"], w["edge_factor"], seed=w["seed"])
+    elif w["kind"] == "copy":
+        g = L.HostGraph.copy_model(w["n"], w["out_degree"], seed=w["seed"])
     else:
         g = L.HostGraph.road(w["width"], w["height"], seed=w["seed"])
     g.compress(w["small_thresh"], 128)
     return g
+
+
+def build_batch(w: dict):
+    """The batched workload's graphs (seeded; seed + i for graph i)."""
+    import lpa_b200 as L
+
+    rng = np.random.default_rng(w["seed"])
+    graphs = []
+    for i in range(w["graphs"]):
+        n = int(np.exp(rng.uniform(np.log(w["n_lo"]), np.log(w["n_hi"]))))
+        if i % 2 == 0:
+            side = max(4, int(round(np.sqrt(n))))
+            g = L.HostGraph.road(side, side, seed=w["seed"] + i)
+        else:
+            g = L.HostGraph.rmat(max(8, int(np.ceil(np.log2(n)))), 8.0, seed=w["seed"] + i, n_limit=n)
+        g.compress(w["small_thresh"], 128)
+        graphs.append(g)
+    return graphs
+
+
+def algorithmic_bytes(arr: dict) -> int:
+    """One iteration's compulsory bytes of one graph (see lpa_info)."""
+    n, n_c = arr["n"], arr["n_c"]
+    return ((int(arr["offsets"][-1]) + 7) // 8 + 8 * (n_c + 1) + 4 * n_c + 4 * (n - n_c + 1)
+            + 4 * len(arr["small_graph"]) + 12 * n)
+
+
+def run_batch(args, w, rank, world, local):
+    """Batched graphs: a step is one persistent launch running every graph to
+    convergence (<= iters iterations)."""
+    import torch
+
+    import lpa_b200 as L
+
+    device = f"cuda:{local}"
+    graphs = build_batch(w)
+    arrs = [g.arrays() for g in graphs]
+    arcs = [int(len(a["small_graph"])) for a in arrs]
+    stream = torch.cuda.Stream(device=device)
+    with L.Batch(graphs, device=local, cms_threshold=w["cms"], stream=stream.cuda_stream) as bt:
+        degs = []
+        for g in graphs:  # arcs per graph from the host CSR
+            row, _ = g.csr()
+            degs.append(int(row[-1]))
+        for _ in range(args.warmup):
+            iters = bt.run(w["iters"], early_exit=True)
+        barrier(world, device)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        total_ms = 0.0
+        work = 0
+        bytes_done = 0
+        wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            ev0.record(stream)
+            iters = bt.run(w["iters"], early_exit=True)
+            ev1.record(stream)
+            ev1.synchronize()
+            total_ms += ev0.elapsed_time(ev1)
+            work += sum(int(d) * int(k) for d, k in zip(degs, iters))
+            bytes_done += sum(algorithmic_bytes(a) * int(k) for a, k in zip(arrs, iters))
+        wall = time.perf_counter() - wall0
+        clk = clocks.stop()
+        total_ms = max_over_ranks(total_ms, world, device)
+        value = work * world / (total_ms / 1e3)
+        # end to end: a run plus every graph's labels back to pinned host memory
+        outs = [torch.empty(a["n"], dtype=torch.int32, pin_memory=True) for a in arrs]
+        lib = L.lib()
+        import ctypes as C
+
+        e0 = time.perf_counter()
+        for _ in range(max(1, args.e2e_steps)):
+            it_e = bt.run(w["iters"], early_exit=True)
+            for gi, o in enumerate(outs):
+                assert lib.lpa_batch_get_labels(bt._h, gi, C.cast(C.c_void_p(o.data_ptr()), C.POINTER(C.c_uint32)),
+                                                arrs[gi]["n"]) == 0
+        e2e_s = max_over_ranks(time.perf_counter() - e0, world, device)
+        e2e_work = sum(int(d) * int(k) for d, k in zip(degs, it_e)) * max(1, args.e2e_steps)
+    peak, peak_kind = measured_peak_gbs()
+    achieved = bytes_done / (total_ms / 1e3) / 1e9
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+                "config": {"workload": args.workload, "graphs": len(graphs), "vertices": int(sum(a["n"] for a in arrs)),
+                           "arcs": int(sum(degs)), "iterations_per_graph": [int(k) for k in iters][:8] + ["..."],
+                           "l2": "inputs larger than L2" if sum(algorithmic_bytes(a) for a in arrs) > 2 * L2_BYTES
+                           else "resident", "parallelism": f"replicas x{world}"},
+                "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_source": peak_kind, "traffic": None},
+                "cpu_baseline": None,
+                "e2e": {"value": e2e_work * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": int(4 * sum(a["n"] for a in arrs))},
+                "gpu_launches": 2 * args.steps, "clocks": clk, "wall_s_timed": wall}
+        print(json.dumps(line), flush=True)
 
 
 def shared_graph_arrays(name: str, w: dict, rank: int, world: int, device=None) -> dict:
@@ -252,6 +357,14 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=torch.device(device))
+
+    if w["kind"] == "batch":
+        run_batch(args, w, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
 
     import lpa_b200 as L
 

@@ -17,6 +17,7 @@ using namespace lpa_dev;
 struct lpa_batch {
   int device = 0;
   cudaStream_t stream = nullptr;
+  bool own_stream = true;
   lpa_opts opts{};
   int num_sms = 148, occ = 1;
   std::vector<uint64_t> n, n_c;
@@ -54,7 +55,7 @@ void free_batch(lpa_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
   for (void *p : b->allocs) cudaFree(p);
-  if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
   cudaGetLastError();
   delete b;
 }
@@ -90,7 +91,12 @@ lpa_status lpa_batch_create(const lpa_graph_desc *graphs, size_t num_graphs, con
     if (b->opts.device < 0 || b->opts.device >= count) throw LPA_ERR_INVALID_ARG;
     b->device = b->opts.device;
     bcheck(cudaSetDevice(b->device));
-    bcheck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    if (b->opts.stream) {
+      b->stream = static_cast<cudaStream_t>(b->opts.stream);
+      b->own_stream = false;
+    } else {
+      bcheck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    }
     bcheck(cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device));
     bcheck(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)));
     bcheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occ, k_batch, kThreads, kSmemBytes));
