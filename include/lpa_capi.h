@@ -180,6 +180,28 @@ lpa_status lpa_get_learned_plan(struct lpa_handle *h, uint8_t *plan, float *pred
 /* Device cycles per segment of the last iteration that recorded them. */
 lpa_status lpa_get_segment_cycles(struct lpa_handle *h, uint64_t *cycles, size_t count);
 
+/* ------------------------------------------------ no-allocation path ----- */
+/* One synchronous iteration (the two-pass path: decode to a CSR, then count)
+ * that allocates nothing, for callers that cannot call cudaMalloc -- a fixed
+ * device-memory budget already spent, buffers owned by the caller's own pool,
+ * or a context where allocation is not allowed.  No counterpart in the
+ * reference.
+ *   g          : every pointer in it is DEVICE memory owned by the caller; the
+ *                stream words need at least 4 zero words after the last bit.
+ *   labels_in / labels_out : device, n entries each, distinct buffers; every
+ *                vertex's output is written.
+ *   stream     : cudaStream_t (NULL: the legacy default stream).
+ *   changed_out: host, may be NULL.
+ * Working memory is one static 16 MiB device array inside the library, held
+ * by every GPU that loads it.  Limits: degrees (n), offsets (n_c + 1) and the
+ * decoded ids of the compressed positions must fit in it, and every degree
+ * must be <= 1023 and below cms_threshold (when non-zero); otherwise the call
+ * returns LPA_ERR_CAPACITY without launching the decode.  The first call on a
+ * device looks up the array's address; make it before any stream capture.
+ * Calls whose work overlaps on the GPU race on the shared array. */
+lpa_status lpa_iterate_noalloc(const lpa_graph_desc *g, const uint32_t *labels_in, uint32_t *labels_out,
+                               uint32_t cms_threshold, void *stream, uint64_t *changed_out);
+
 /* ------------------------------------------ host format layer (lpa_hg_*) --- */
 /* A host graph owns a CSR (by vertex id) and/or its compressed form, produced
  * by the fast bit-identical encoder that replaces CgrCompressor

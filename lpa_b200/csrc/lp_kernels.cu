@@ -20,6 +20,7 @@
 // Every loop is bounded by the bits it consumes; malformed input sets the
 // error word instead of trapping.
 #include "lp_kernels.cuh"
+#include "noalloc.cuh"
 
 namespace lpa_dev {
 
@@ -1166,5 +1167,7 @@ __global__ void k_init_labels(uint32_t *a, uint32_t *b, uint64_t n) {
     b[v] = uint32_t(v);
   }
 }
+
+#include "noalloc_kernels.cuh"  // kernels of lpa_iterate_noalloc
 
 }  // namespace lpa_dev
