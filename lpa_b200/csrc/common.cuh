@@ -378,9 +378,11 @@ struct EpochTable {
   unsigned long long *slots;
   uint32_t cap;
   uint32_t epoch;  // 1..65535
+  // Triangular probing (h, h+1, h+3, h+6, ...) visits every slot of a
+  // power-of-two table and keeps probe chains short at high load.
   __device__ __forceinline__ uint32_t insert(uint32_t label, uint32_t c) const {
     const unsigned long long tag = (uint64_t(epoch) << 48) | (uint64_t(label) << 16);
-    uint32_t h = slot_hash(label) & (cap - 1);
+    uint32_t h = slot_hash(label) & (cap - 1), step = 0;
     for (uint32_t probe = 0; probe < 2 * cap; probe++) {
       const unsigned long long v = slots[h];
       if (uint32_t(v >> 48) == epoch) {
@@ -388,7 +390,7 @@ struct EpochTable {
           const unsigned long long old = atomicAdd(&slots[h], (unsigned long long)c);
           return uint32_t(old & 0xFFFFull) + c;
         }
-        h = (h + 1) & (cap - 1);
+        h = (h + ++step) & (cap - 1);
         continue;
       }
       if (atomicCAS(&slots[h], v, tag | c) == v) return c;
@@ -397,6 +399,53 @@ struct EpochTable {
     return 0;
   }
 };
+
+// Folds lanes holding equal labels into one lane: returns the number of lanes
+// folded into this one (0 for a lane folded into another, or when !ok).  Each
+// round folds every lane equal to the lowest unfolded lane's label (one
+// shuffle, one ballot), so a warp whose lanes share a few labels ends with a
+// few weighted lanes.  Rounds stop after four, or after a round that folded a
+// single lane; the lanes left keep weight 1.  Called by all 32 lanes.
+__device__ __forceinline__ uint32_t warp_merge(bool ok, uint32_t lab) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t rest = __ballot_sync(0xFFFFFFFFu, ok);
+  uint32_t w = ok ? 1u : 0u;
+  for (int r = 0; r < 4 && rest; r++) {
+    const uint32_t ld = uint32_t(__ffs(rest) - 1);
+    const uint32_t x = __shfl_sync(0xFFFFFFFFu, lab, ld);
+    const uint32_t eq = __ballot_sync(0xFFFFFFFFu, ((rest >> lane) & 1u) && lab == x);
+    if ((eq >> lane) & 1u) w = (lane == ld) ? uint32_t(__popc(eq)) : 0u;
+    rest &= ~eq;
+    if (__popc(eq) == 1) break;
+  }
+  return w;
+}
+
+// For every lane, how many lanes of its group (gm: the group's lane mask, gl:
+// the group index, groups of a power-of-two size) hold its label; 0 when !ok.
+// Two ballot rounds settle the groups' most common labels; lanes left after
+// them are counted with match.any.  Called by all 32 lanes.
+__device__ __forceinline__ uint32_t group_counts(bool ok, uint32_t lab, uint32_t gm, uint32_t gl) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t rest = __ballot_sync(0xFFFFFFFFu, ok);
+  uint32_t cnt = 0;
+  for (int r = 0; r < 2 && rest; r++) {
+    const uint32_t mine = rest & gm;
+    const uint32_t ld = mine ? uint32_t(__ffs(mine) - 1) : lane;
+    const uint32_t x = __shfl_sync(0xFFFFFFFFu, lab, ld);
+    const bool hit = ((mine >> lane) & 1u) && lab == x;
+    const uint32_t hits = __ballot_sync(0xFFFFFFFFu, hit);
+    if (hit) cnt = uint32_t(__popc(hits & gm));
+    rest &= ~hits;
+  }
+  if (rest) {
+    const bool rem = (rest >> lane) & 1u;
+    const unsigned long long key = rem ? ((uint64_t(gl) << 32) | lab) : (0xFFFFFFFF00000000ull | lane);
+    const uint32_t m = __match_any_sync(0xFFFFFFFFu, key);
+    if (rem) cnt = uint32_t(__popc(m));
+  }
+  return cnt;
+}
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 

@@ -104,13 +104,13 @@ __device__ __forceinline__ uint32_t block_scan(BlockSh &sh, uint32_t v) {
 
 // ------------------------------------------------------------ consumers ---
 // Called warp-synchronously by every lane; ok marks a real label.  Lanes of a
-// warp holding the same label are merged first (match.any), so each distinct
-// label of a step touches the table once.
+// warp holding the same label are folded first (warp_merge), so a step whose
+// lanes share a label touches the table once.
 struct ExactSink {  // global table (key/count arrays, cleared after use)
   uint32_t *keys, *cnts, cap;
   __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
-    const uint32_t m = __match_any_sync(kFull, ok ? lab : kFull);
-    if (ok && (__ffs(m) - 1) == int(threadIdx.x & 31u)) table_add(keys, cnts, cap, lab, __popc(m));
+    const uint32_t w = warp_merge(ok, lab);
+    if (w) table_add(keys, cnts, cap, lab, w);
   }
 };
 
@@ -118,9 +118,9 @@ struct EpochSink {  // shared epoch table with a running argmax per thread
   EpochTable et;
   uint64_t *best;
   __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
-    const uint32_t m = __match_any_sync(kFull, ok ? lab : kFull);
-    if (ok && (__ffs(m) - 1) == int(threadIdx.x & 31u)) {
-      const uint64_t cand = pack_best(et.insert(lab, __popc(m)), lab);
+    const uint32_t w = warp_merge(ok, lab);
+    if (w) {
+      const uint64_t cand = pack_best(et.insert(lab, w), lab);
       if (cand > *best) *best = cand;
     }
   }
@@ -130,23 +130,22 @@ struct CmsAddSink {
   uint32_t *cms;
   const uint32_t *seeds;
   __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
-    const uint32_t m = __match_any_sync(kFull, ok ? lab : kFull);
-    if (ok && (__ffs(m) - 1) == int(threadIdx.x & 31u)) {
-      const uint32_t c = __popc(m);
+    const uint32_t w = warp_merge(ok, lab);
+    if (w) {
 #pragma unroll
       for (int r = 0; r < kCmsDepth; r++)
-        atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, lab ^ seeds[r]) & (kCmsWidth - 1))], c);
+        atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, lab ^ seeds[r]) & (kCmsWidth - 1))], w);
     }
   }
 };
 
+// Second sketch pass: read-only, so every lane looks up its own label.
 struct CmsBestSink {
   const uint32_t *cms;
   const uint32_t *seeds;
   uint64_t *best;
   __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
-    const uint32_t m = __match_any_sync(kFull, ok ? lab : kFull);
-    if (ok && (__ffs(m) - 1) == int(threadIdx.x & 31u)) {
+    if (ok) {
       uint32_t est = kFull;
 #pragma unroll
       for (int r = 0; r < kCmsDepth; r++) {
@@ -159,15 +158,16 @@ struct CmsBestSink {
   }
 };
 
-// Labels of the global ids src[0..total) into stage.
+// Labels of the global ids src[0..total) into stage (src_labels: src holds
+// the labels themselves).
 __device__ __forceinline__ void block_gather_from(uint32_t *stage, const uint32_t *__restrict__ src, uint32_t total,
-                                                  const Ctx &c) {
+                                                  const Ctx &c, bool src_labels) {
   for (uint32_t k0 = threadIdx.x; k0 < total; k0 += 4 * kThreads) {
     uint32_t v[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const uint32_t k = k0 + u * kThreads;
-      v[u] = k < total ? ld_label(c, __ldg(src + k)) : 0u;
+      v[u] = k >= total ? 0u : (src_labels ? __ldcs(src + k) : ld_label(c, __ldg(src + k)));
     }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
@@ -195,11 +195,12 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
   const DevGraph &g = a.g;
   const uint32_t t = threadIdx.x;
   if (p >= g.n_c || from_scratch) {
-    // contiguous ids: the small CSR, or the two-pass scratch
-    const uint32_t *src = (p >= g.n_c) ? g.small_nbr + g.small_off[p - g.n_c] : a.scratch + a.arc_off[p];
+    // contiguous: the small CSR's ids, or the labels the two-pass pre-pass wrote
+    const bool labels = p < g.n_c && a.scratch_labels;
+    const uint32_t *src = labels ? a.scratch + a.arc_off[p] : g.small_nbr + g.small_off[p - g.n_c];
     for (uint32_t c0 = 0; c0 < d; c0 += kStage) {
       const uint32_t cnt = min(kStage, d - c0);
-      block_gather_from(stage, src + c0, cnt, c);
+      block_gather_from(stage, src + c0, cnt, c, labels);
       __syncthreads();
       block_consume_stage(stage, cnt, sink);
       __syncthreads();
@@ -406,6 +407,7 @@ __device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint3
   const uint32_t node = g.vertices[p];
   const uint32_t d = g.deg[p];
   const uint32_t old = ld_label(c, node);
+  if (a.cursor && from_scratch && p < g.n_c && t == 0) a.cursor[p] = 0u;  // the pre-pass's output cursor, for the next iteration
   if (d == 0) return;
   uint64_t best = 0;
   if (a.cms_thr != 0 && d >= a.cms_thr) {
@@ -623,6 +625,7 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, un
   const uint32_t old = valid ? ld_label(c, node) : 0u;
   const bool cgr = p0 < g.n_c;  // chunks never straddle the compressed / small boundary
   const bool decode = cgr && variant != kVarTwoPass;
+  if (a.cursor && cgr && !decode && valid) a.cursor[p] = 0u;  // the pre-pass's output cursor, for the next iteration
   if (d > cap_stage || (variant == kVarPacked && d > kV2MaxDeg) || d > kV1MaxDeg) {
     set_error(a.err, kErrCapacity);
     d = 0;
@@ -652,7 +655,10 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, un
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const uint32_t k = k0 + 32 * u;
-        v[u] = k < total ? ld_label(c, decode ? stage[k] : __ldg(src + src_skip + k)) : 0u;
+        v[u] = k >= total ? 0u
+                          : (decode ? ld_label(c, stage[k])
+                                    : (cgr && a.scratch_labels ? __ldcs(src + src_skip + k)
+                                                               : ld_label(c, __ldg(src + src_skip + k))));
       }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
@@ -679,8 +685,7 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, un
         const uint32_t oldv = __shfl_sync(kFull, old, srcl);
         const bool ok = vin && k < dv;
         const uint32_t lab = ok ? stage[bv + k] : kFull;
-        const uint32_t m = __match_any_sync(kFull, (uint64_t(gl) << 32) | lab);
-        const uint32_t cnt = ok ? __popc(m) : 0u;
+        const uint32_t cnt = group_counts(ok, lab, gm, gl);
         const uint32_t maxc = __reduce_max_sync(gm, cnt);
         const uint32_t bestl = __reduce_min_sync(gm, (ok && cnt == maxc) ? lab : kFull);
         if (vin && k == 0) {
@@ -700,8 +705,7 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, un
         if (dv <= 32) {
           const bool ok = lane < dv;
           const uint32_t lab = ok ? stage[bv + lane] : kFull;
-          const uint32_t m = __match_any_sync(kFull, lab);
-          const uint32_t cnt = ok ? __popc(m) : 0u;
+          const uint32_t cnt = group_counts(ok, lab, kFull, 0u);
           const uint32_t maxc = __reduce_max_sync(kFull, cnt);
           bestl = __reduce_min_sync(kFull, (ok && cnt == maxc) ? lab : kFull);
         } else {
@@ -717,9 +721,9 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, un
             const uint32_t k = k0 + lane;
             const bool ok = k < dv;
             const uint32_t lab = ok ? stage[bv + k] : kFull;
-            const uint32_t m = __match_any_sync(kFull, lab);
-            if (ok && (__ffs(m) - 1) == int(lane)) {
-              const uint64_t cand = pack_best(et.insert(lab, __popc(m)), lab);
+            const uint32_t w = warp_merge(ok, lab);
+            if (w) {
+              const uint64_t cand = pack_best(et.insert(lab, w), lab);
               bp = cand > bp ? cand : bp;
             }
           }
@@ -880,6 +884,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchArgs b) {
       for (int r = 0; r < kCmsDepth; r++) ia.seeds[r] = b.seeds[r];
       ia.scratch = nullptr;
       ia.arc_off = nullptr;
+      ia.scratch_labels = 0;
+      ia.groups = nullptr;
+      ia.n_groups = 0;
+      ia.pidx = nullptr;
+      ia.cursor = nullptr;
       ia.gtab = b.gtab;
       ia.gtab_slots = b.gtab_slots;
     }
@@ -943,164 +952,172 @@ __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs) {
   }
 }
 
-// Two-pass variant, pass 1: the two-pass segments' compressed positions are
-// decoded into the scratch CSR.  Light segments: one warp per 32-position
-// chunk with the segment-parallel warp decoder.  Single hub vertices: the
-// block decodes 256 residual segments per round (one thread each) at offsets
-// from a block prefix sum, after expanding the interval section.
+// Two-pass variant, pass 1.  Every 256-bit segment of the two-pass positions
+// is decoded by one lane, which writes the labels of its ids (not the ids) to
+// the scratch, so pass 2 only counts.  A warp takes one decode group (32
+// segments).  Lane l finds its position with a warp scan of the positions'
+// segment counts and a 5-step search; the lanes of one position reserve their
+// output range with one atomicAdd on the position's cursor, since the labels
+// of a position may sit in any order.  No block barriers: warps run alone.
 __global__ void __launch_bounds__(kThreads) k_decode_two_pass(IterArgs a) {
-  __shared__ BlockSh sh;
   const DevGraph &g = a.g;
-  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
-  for (uint32_t i = blockIdx.x; i < a.n_two_pass; i += gridDim.x) {
-    const uint32_t s = a.two_pass[i];
-    const Seg sg = a.segs[s];
-    if (sg.begin >= g.n_c) continue;
+  const Ctx c = resolve(a);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < a.n_groups; gi += nw) {
     const long long t0 = clock64();
-    const bool hub = sg.end - sg.begin == 1 && g.deg[sg.begin] > kV1MaxDeg;
-    if (!hub) {
-      const uint32_t nchunks = (sg.end - sg.begin + 31) / 32;
-      for (uint32_t ch = warp; ch < nchunks; ch += kWarps) {
-        const uint32_t p0 = sg.begin + ch * 32;
-        const uint32_t p = p0 + lane;
-        const bool valid = p < sg.end;
-        const uint32_t node = valid ? g.vertices[p] : 0u;
-        const uint32_t d = valid ? g.deg[p] : 0u;
-        const uint64_t o0 = a.arc_off[p0];
-        const uint32_t base = valid ? uint32_t(a.arc_off[p] - o0) : 0u;
-        if (!warp_decode_batch(g, a.scratch + o0, valid, p, node, d, base, lane) && lane == 0)
-          set_error(a.err, kErrBadStream);
+    const DecodeGroup gd = a.groups[gi];
+    const uint32_t pk = gd.p0 + lane;
+    uint4 ix = make_uint4(0u, 0u, 0u, 0u);
+    if (pk < g.n_c) ix = a.pidx[pk];
+    uint32_t ns = ix.z + ix.w;
+    if (lane == 0) ns = ns > gd.j0 ? ns - gd.j0 : 0u;
+    const uint32_t incl = warp_incl_scan(ns, lane);
+    const uint32_t total = min(__shfl_sync(kFull, incl, 31), min(gd.nlanes, 32u));
+    // owner: the number of positions whose segments all precede this lane
+    uint32_t o = 0;
+#pragma unroll
+    for (uint32_t st = 16; st; st >>= 1) {
+      const uint32_t v = __shfl_sync(kFull, incl, o + st - 1);
+      if (v <= lane) o += st;
+    }
+    const uint32_t os = o & 31u;
+    const uint32_t run0 = __shfl_sync(kFull, incl - ns, os);  // first lane of this position's run
+    const uint32_t run1 = min(__shfl_sync(kFull, incl, os), total);
+    const uint32_t ibr = __shfl_sync(kFull, ix.x, os), rbr = __shfl_sync(kFull, ix.y, os);
+    const uint32_t nsi = __shfl_sync(kFull, ix.z, os);
+    const bool act = lane < total;
+    const uint32_t p = gd.p0 + os;
+    const uint32_t jj = lane - run0 + (os == 0 ? gd.j0 : 0u);
+    const bool itv = jj < nsi;
+    bool bad = false;
+    uint32_t cnt = 0, items = 0, node = 0;
+    uint64_t q = 0, end = 0;
+    BitReader r;
+    if (act) {
+      const uint64_t o0 = g.offsets[p];
+      end = g.offsets[p + 1];
+      node = g.vertices[p];
+      q = o0 + (itv ? uint64_t(ibr) + uint64_t(kSegBits) * jj : uint64_t(rbr) + uint64_t(kSegBits) * (jj - nsi));
+      if (q >= end) {
+        bad = true;
+      } else {
+        r.seek(g.words, q);
+        cnt = r.gamma(bad);
+        if (!itv) {
+          items = cnt;
+        } else {
+          for (uint32_t k = 0; k < cnt && !bad; k++) {
+            r.gamma(bad);
+            items += r.gamma(bad) + kMinItv;
+            if (r.pos > end) bad = true;
+          }
+        }
       }
-    } else {
-      const uint32_t p = sg.begin;
-      const uint32_t node = g.vertices[p];
+      if (bad) {
+        cnt = 0;
+        items = 0;
+      }
+    }
+    // output ranges: exclusive scan of items within the position's run
+    const uint32_t iincl = warp_incl_scan(items, lane);
+    const uint32_t run_before = __shfl_sync(kFull, iincl - items, run0 & 31u);
+    const uint32_t run_total = __shfl_sync(kFull, iincl, (run1 - 1) & 31u) - run_before;
+    uint32_t base = 0;
+    if (act && lane == run0 && run_total) base = atomicAdd(a.cursor + p, run_total);
+    base = __shfl_sync(kFull, base, run0 & 31u);
+    if (act) {
       const uint32_t d = g.deg[p];
-      uint32_t *out = a.scratch + a.arc_off[p];
-      const uint64_t end = g.offsets[p + 1];
-      bool bad = false;
-      if (t == 0) {
-        BitReader r;
-        r.seek(g.words, g.offsets[p]);
-        uint32_t ns = r.segcnt(bad);
-        if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
-          bad = true;
-          ns = 0;
-        }
-        sh.nseg_i = ns;
-        sh.ibase = r.pos;
-        sh.last_end = r.pos;
-        sh.items = 0;
-        sh.bad = bad ? 1u : 0u;
-      }
-      __syncthreads();
-      const uint32_t nseg_i = sh.nseg_i;
-      uint32_t written = 0;  // block-uniform item cursor
-      for (uint32_t j0 = 0; j0 < nseg_i; j0 += kThreads) {
-        const uint32_t j = j0 + t;
-        bool has = j < nseg_i;
-        BitReader r;
-        uint32_t cnt = 0, cc = 0, left = 0;
-        const uint64_t q = sh.ibase + uint64_t(kSegBits) * j;
-        if (has) {
-          if (q >= end) {
-            bad = true;
-            has = false;
-          } else {
-            r.seek(g.words, q);
-            cnt = r.gamma(bad);
+      const uint32_t off = base + (iincl - items) - run_before;
+      if (uint64_t(off) + items > d) {
+        bad = true;
+      } else if (items) {
+        uint32_t *out = a.scratch + a.arc_off[p] + off;
+        if (!itv) {
+          uint32_t v = 0;
+          for (uint32_t k = 0; k < cnt; k += 4) {
+            uint32_t ids[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+              ids[u] = node;
+              if (k + u < cnt) {
+                const uint32_t x = r.zeta3(bad);
+                v = (k + u == 0) ? zigzag_first(node, x) : v + x + 1u;
+                ids[u] = v;
+                if (bad || r.pos > end || uint64_t(v) >= g.n) {
+                  bad = true;
+                  ids[u] = node;  // in range; the error word reports the stream
+                }
+              }
+            }
+            uint32_t lv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) lv[u] = (k + u < cnt) ? ld_label(c, ids[u]) : 0u;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+              if (k + u < cnt) out[k + u] = lv[u];
           }
-        }
-        while (__syncthreads_or(has && cc < cnt)) {
-          uint32_t len = 0;
-          if (has && cc < cnt) {
+        } else {
+          r.seek(g.words, q);
+          r.gamma(bad);
+          uint32_t left = 0, w = 0;
+          for (uint32_t k = 0; k < cnt; k++) {
             const uint32_t l = r.gamma(bad);
-            left = (cc == 0) ? zigzag_first(node, l) : left + l + 1u;
-            len = r.gamma(bad) + kMinItv;
-            cc++;
-            if (bad || r.pos > end || uint64_t(left) + len > g.n) {
-              bad = true;
-              len = 0;
-              cnt = cc;
-            }
-          }
-          sh.left[t] = left;
-          const uint32_t total = block_scan(sh, len);
-          if (len) left += len;
-          for (uint32_t i0 = t; i0 < total; i0 += kThreads) {
-            uint32_t lo = 0, hi = kThreads - 1;
-            while (lo < hi) {
-              const uint32_t mid = (lo + hi + 1) >> 1;
-              if (sh.pref[mid] <= i0) lo = mid;
-              else hi = mid - 1;
-            }
-            if (written + i0 < d) out[written + i0] = sh.left[lo] + (i0 - sh.pref[lo]);
-          }
-          written += total;
-          __syncthreads();
-        }
-        if (has && j == nseg_i - 1) sh.last_end = r.pos;
-      }
-      __syncthreads();
-      if (t == 0) {
-        BitReader r;
-        r.seek(g.words, sh.last_end);
-        uint32_t ns = r.segcnt(bad);
-        if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
-          bad = true;
-          ns = 0;
-        }
-        sh.nseg_r = ns;
-        sh.rbase = r.pos;
-        sh.last_end = r.pos;
-      }
-      __syncthreads();
-      const uint32_t nseg_r = sh.nseg_r;
-      for (uint32_t j0 = 0; j0 < nseg_r; j0 += kThreads) {
-        const uint32_t j = j0 + t;
-        bool has = j < nseg_r;
-        BitReader r;
-        uint32_t cnt = 0;
-        if (has) {
-          const uint64_t q = sh.rbase + uint64_t(kSegBits) * j;
-          if (q >= end) {
-            bad = true;
-            has = false;
-          } else {
-            r.seek(g.words, q);
-            cnt = r.gamma(bad);
-            if (bad) cnt = 0;
-          }
-        }
-        const uint32_t total = block_scan(sh, cnt);
-        if (has) {
-          uint32_t o = written + sh.pref[t], v = 0;
-          for (uint32_t cc = 0; cc < cnt; cc++) {
-            const uint32_t x = r.zeta3(bad);
-            v = (cc == 0) ? zigzag_first(node, x) : v + x + 1u;
-            if (bad || r.pos > end || uint64_t(v) >= g.n || o >= d) {
+            left = (k == 0) ? zigzag_first(node, l) : left + l + 1u;
+            const uint32_t len = r.gamma(bad) + kMinItv;
+            if (bad || uint64_t(left) + len > g.n || w + len > items) {
               bad = true;
               break;
             }
-            out[o++] = v;
+            for (uint32_t e = 0; e < len; e++) out[w + e] = ld_label(c, left + e);
+            w += len;
+            left += len;
           }
-          if (j == nseg_r - 1) sh.last_end = r.pos;
         }
-        written += total;
-        __syncthreads();
       }
-      if (bad) sh.bad = 1;
-      __syncthreads();
-      if (sh.bad || sh.last_end != end || written != d) {
-        // keep every scratch id in range; the error word reports the stream
-        for (uint32_t k = t; k < d; k += kThreads) out[k] = node;
-        if (t == 0) set_error(a.err, kErrBadStream);
-      }
-      __syncthreads();
     }
-    if (a.seg_cycles && t == 0)
-      atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s),
-                (unsigned long long)((clock64() - t0) * kWarps));
-    __syncthreads();
+    if (__any_sync(kFull, bad) && lane == 0) set_error(a.err, kErrBadStream);
+    if (a.seg_cycles && lane == 0)
+      atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + gd.seg), (unsigned long long)(clock64() - t0));
+  }
+}
+
+__global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err) {
+  for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < g.n_c;
+       p += uint64_t(gridDim.x) * blockDim.x) {
+    bool bad = false;
+    const uint64_t o0 = g.offsets[p], end = g.offsets[p + 1];
+    BitReader r;
+    r.seek(g.words, o0);
+    const uint32_t nsi = r.segcnt(bad);
+    const uint64_t ibase = r.pos;
+    uint64_t last = r.pos;
+    if (!bad && nsi && ibase + uint64_t(kSegBits) * (nsi - 1) < end) {
+      // only the last interval segment is unpadded: decode it to find its end
+      BitReader q;
+      q.seek(g.words, ibase + uint64_t(kSegBits) * (nsi - 1));
+      const uint32_t cnt = q.gamma(bad);
+      for (uint32_t k = 0; k < cnt && !bad && q.pos <= end; k++) {
+        q.gamma(bad);
+        q.gamma(bad);
+      }
+      last = q.pos;
+    } else if (nsi) {
+      bad = true;
+    }
+    uint32_t nsr = 0;
+    uint64_t rbase = last;
+    if (!bad && last <= end) {
+      r.seek(g.words, last);
+      nsr = r.segcnt(bad);
+      rbase = r.pos;
+    }
+    if (bad || rbase > end || rbase - o0 > 0xFFFFFFFFull || (nsr && rbase + uint64_t(kSegBits) * (nsr - 1) >= end)) {
+      set_error(err, kErrBadStream);
+      pidx[p] = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+      pidx[p] = make_uint4(uint32_t(ibase - o0), uint32_t(rbase - o0), nsi, nsr);
+    }
   }
 }
 

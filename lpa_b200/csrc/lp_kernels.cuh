@@ -41,6 +41,14 @@ struct WorkItem {
   uint64_t pf_addr;    // device address of the range (bitstream bits, small-CSR ids or scratch ids)
 };
 
+// Work of the two-pass pre-pass: nlanes (<= 32) consecutive segments of the
+// positions p0, p0 + 1, ..., starting at segment j0 of p0 (interval segments
+// first, then residual ones) and spanning at most 32 positions.  seg is the
+// plan segment its cycles are booked to.
+struct DecodeGroup {
+  uint32_t p0, j0, nlanes, seg;
+};
+
 struct IterArgs {
   DevGraph g;
   uint32_t *labs0, *labs1;      // the two label buffers
@@ -55,15 +63,20 @@ struct IterArgs {
   uint32_t n_heavy;
   const WorkItem *light;        // warp work items (32-position chunks)
   uint32_t n_light;
-  const uint32_t *two_pass;     // segments decoded by the two-pass pre-pass
-  uint32_t n_two_pass;
+  const DecodeGroup *groups;    // two-pass pre-pass work: 32 segments per group
+  uint32_t n_groups;
+  const uint4 *pidx;            // per compressed position: {ibase - offset, rbase - offset, nseg_i, nseg_r}
+  uint32_t *cursor;             // per compressed position: labels written by the pre-pass (pass 2 resets)
   long long *seg_cycles;        // per-segment device cycles (nullptr: off)
   uint32_t *seg_changed;        // per-segment changed counts (nullptr: off)
   uint32_t cms_thr;             // 0: no sketch
   uint32_t seeds[kCmsDepth];
-  // two-pass scratch: ids of compressed position p at scratch[arc_off[p]..)
+  // two-pass scratch: the neighbours of compressed position p at
+  // scratch[arc_off[p]..), as labels in any order (k_decode_two_pass) or as
+  // ids (scratch_labels == 0)
   uint32_t *scratch;
   const uint64_t *arc_off;
+  uint32_t scratch_labels;      // 1: the scratch holds labels (the pre-pass), 0: ids
   // global exact-count tables for exact vertices above kBlockMaxSmemDeg
   uint32_t *gtab;
   uint32_t gtab_slots;          // slots per block (power of two), 0: none
@@ -118,6 +131,10 @@ struct DecodeArgs {
   uint32_t *err;
 };
 __global__ void k_decode_positions(DecodeArgs a);
+
+// Per compressed position: where its interval and residual sections'
+// segments start (relative to its bit offset) and how many each has.
+__global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err);
 
 __global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *itv_out, uint32_t *err);
 __global__ void k_init_labels(uint32_t *a, uint32_t *b, uint64_t n);

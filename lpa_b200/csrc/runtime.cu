@@ -211,7 +211,7 @@ static void upload_lists(lpa_handle *h) {
   // items: 32-position chunks of the others; two-pass segments of the
   // compressed region are decoded by the pre-pass.
   std::vector<WorkItem> heavy, light;
-  std::vector<uint32_t> two;
+  std::vector<DecodeGroup> groups;
   for (size_t s = 0; s < h->segs.size(); s++) {
     const int v = h->variant[s];
     const SegInfo &si = h->segs[s];
@@ -226,14 +226,36 @@ static void upload_lists(lpa_handle *h) {
         light.push_back(make_item(h, (uint32_t(s) << 3) | c, p0, p1, tp));
       }
     }
-    if (tp && si.region == 0) two.push_back(uint32_t(s));
+    if (tp && si.region == 0) {
+      // decode groups: 32 consecutive segments of the positions, spanning at
+      // most 32 positions (every lane of the pre-pass finds its position
+      // among the 32 it loads)
+      uint32_t p = si.begin, j = 0;
+      while (p < si.end) {
+        DecodeGroup gd{p, j, 0, uint32_t(s)};
+        uint32_t positions = 0;
+        while (p < si.end && gd.nlanes < 32 && positions < 32) {
+          const uint32_t ns = h->h_nseg[p];
+          const uint32_t take = std::min(ns - j, 32u - gd.nlanes);
+          gd.nlanes += take;
+          positions++;
+          if (j + take == ns) {
+            p++;
+            j = 0;
+          } else {
+            j += take;
+          }
+        }
+        if (gd.nlanes) groups.push_back(gd);
+      }
+    }
   }
   std::stable_sort(heavy.begin(), heavy.end(), [&](const WorkItem &a, const WorkItem &b) {
     return h->segs[a.tag].arcs > h->segs[b.tag].arcs;
   });
   h->n_heavy = uint32_t(heavy.size());
   h->n_light = uint32_t(light.size());
-  h->n_two_pass = uint32_t(two.size());
+  h->n_groups = uint32_t(groups.size());
   std::vector<WorkItem> all;
   all.reserve(heavy.size() + light.size());
   all.insert(all.end(), heavy.begin(), heavy.end());
@@ -249,13 +271,15 @@ static void upload_lists(lpa_handle *h) {
     ptr = dalloc<std::remove_reference_t<decltype(*ptr)>>(h, cap, what);
   };
   regrow(h->d_items, h->items_cap, all.size(), "work items");
-  regrow(h->d_two, h->two_cap, two.size(), "two-pass list");
+  regrow(h->d_groups, h->groups_cap, groups.size(), "decode groups");
   h2d(h, h->d_items, all.data(), all.size(), "upload work items");
-  h2d(h, h->d_two, two.data(), two.size(), "upload two-pass list");
+  h2d(h, h->d_groups, groups.data(), groups.size(), "upload decode groups");
   h2d(h, h->d_seg_var, h->variant.data(), h->variant.size(), "upload variants");
   check(h, cudaStreamSynchronize(h->stream), "upload work lists");
   h->plan_version++;
-  h->grid_decode = int(std::max<uint64_t>(1, std::min<uint64_t>(h->n_two_pass, uint64_t(h->num_sms) * 4)));
+  // one warp per decode group, kThreads / 32 warps per block
+  h->grid_decode = int(std::max<uint64_t>(
+      1, std::min<uint64_t>((uint64_t(h->n_groups) + kWarps - 1) / kWarps, uint64_t(h->num_sms) * 8)));
 }
 
 static void ensure_two_pass_scratch(lpa_handle *h) {
@@ -266,6 +290,23 @@ static void ensure_two_pass_scratch(lpa_handle *h) {
   h->d_arc_off = dalloc<uint64_t>(h, h->n + 1, "arc offsets");
   h2d(h, h->d_arc_off, off.data(), h->n + 1, "upload arc offsets");
   h->d_scratch = dalloc<uint32_t>(h, off[h->n_c], "two-pass scratch");
+  // where every compressed position's segments start, for the pre-pass
+  const uint64_t nc = std::max<uint64_t>(1, h->n_c);
+  h->d_pidx = dalloc<uint4>(h, nc, "position index");
+  h->d_cursor = dalloc<uint32_t>(h, nc, "pre-pass cursors");
+  check(h, cudaMemsetAsync(h->d_cursor, 0, nc * sizeof(uint32_t), h->stream), "clear cursors");
+  if (h->n_c) {
+    const int blocks = int(std::min<uint64_t>((h->n_c + 127) / 128, uint64_t(h->num_sms) * 32));
+    k_pos_index<<<std::max(blocks, 1), 128, 0, h->stream>>>(dev_graph(h), h->d_pidx, h->d_err);
+    check(h, cudaGetLastError(), "position index launch");
+  }
+  lpa_status st = take_device_error(h);
+  if (st != LPA_OK) throw Fail{st, "position index: " + h->last_error};
+  std::vector<uint4> pidx(h->n_c);
+  if (h->n_c)
+    check(h, cudaMemcpy(pidx.data(), h->d_pidx, h->n_c * sizeof(uint4), cudaMemcpyDeviceToHost), "read index");
+  h->h_nseg.resize(h->n_c);
+  for (uint64_t p = 0; p < h->n_c; p++) h->h_nseg[p] = pidx[p].z + pidx[p].w;
   check(h, cudaStreamSynchronize(h->stream), "arc offsets");
 }
 
@@ -367,14 +408,17 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.n_heavy = h->n_heavy;
   a.light = h->d_items + h->n_heavy;
   a.n_light = h->n_light;
-  a.two_pass = h->d_two;
-  a.n_two_pass = h->n_two_pass;
+  a.groups = h->d_groups;
+  a.n_groups = h->n_groups;
+  a.pidx = h->d_pidx;
+  a.cursor = h->d_cursor;
   a.seg_cycles = (h->opts.record_timings >= 2 || h->collect_cycles) ? h->d_seg_cycles : nullptr;
   a.seg_changed = h->learner ? h->d_seg_changed : nullptr;
   a.cms_thr = h->opts.cms_threshold;
   for (int r = 0; r < kCmsDepth; r++) a.seeds[r] = h->seeds[r];
   a.scratch = h->d_scratch;
   a.arc_off = h->d_arc_off;
+  a.scratch_labels = 1;
   a.gtab = h->d_gtab;
   a.gtab_slots = h->gtab_slots;
   return a;
@@ -387,7 +431,7 @@ static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32
   const bool timed = h->opts.record_timings && h->events_ready;
   const IterArgs a = iter_args(h, changed, work);
   if (timed) cudaEventRecord(h->ev[0], h->stream);
-  if (h->n_two_pass) {
+  if (h->n_groups) {
     k_decode_two_pass<<<h->grid_decode, kThreads, 0, h->stream>>>(a);
     h->launches++;
   }

@@ -75,9 +75,12 @@ struct lpa_handle {
   lpa_dev::Seg *d_segs = nullptr;
   uint8_t *d_seg_var = nullptr;
   lpa_dev::WorkItem *d_items = nullptr;  // heavy items | light chunk items
-  uint32_t *d_two = nullptr;              // two-pass segments
-  uint32_t n_heavy = 0, n_light = 0, n_two_pass = 0;
-  size_t items_cap = 0, two_cap = 0;
+  lpa_dev::DecodeGroup *d_groups = nullptr;  // two-pass pre-pass work (32 segments each)
+  uint32_t n_heavy = 0, n_light = 0, n_groups = 0;
+  size_t items_cap = 0, groups_cap = 0;
+  uint4 *d_pidx = nullptr;                   // per compressed position: section starts and segment counts
+  std::vector<uint32_t> h_nseg;              // per compressed position: interval + residual segments
+  uint32_t *d_cursor = nullptr;              // per compressed position: pre-pass output cursor
   std::vector<uint64_t> h_offsets;        // host copies for the prefetch ranges
   std::vector<uint32_t> h_small_off;
   std::vector<uint64_t> h_arc_off;
