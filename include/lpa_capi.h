@@ -109,6 +109,7 @@ typedef struct lpa_stats {
   uint64_t launches;                /* kernel launches enqueued by this handle */
   double decode_ms;                 /* two-pass decode kernel, last iteration */
   double iterate_ms;                /* persistent iteration kernel, last iteration */
+  double count_ms;                  /* two-pass count kernel, last iteration */
 } lpa_stats;
 
 /* ---------------------------------------------------------------- basics -- */
@@ -158,6 +159,13 @@ lpa_status lpa_get_degrees(struct lpa_handle *h, uint32_t *deg_out, size_t n);
 /* Dispatch control.  Assign a variant to one segment (-1: all segments whose
  * degrees it supports), rebuilding the launch lists. */
 lpa_status lpa_set_dispatch(struct lpa_handle *h, int dispatch, int force_variant);
+/* An explicit plan: variant[s] for every segment s (count = lpa_info.num_segments),
+ * e.g. a plan found by a tuner.  A variant a segment cannot run is rejected
+ * (LPA_ERR_INVALID_ARG) and the plan is left as it was.  The handle switches to
+ * LPA_DISPATCH_FORCE semantics (no learning) until the next lpa_set_dispatch.
+ * No counterpart in the reference, which hard-codes its degree buckets
+ * (baselines/novaplus/novaplus_propogator.cuh:219-220). */
+lpa_status lpa_set_plan(struct lpa_handle *h, const uint8_t *variant, size_t count);
 /* Per-segment view of the plan: begin/end positions, bucket, variant. */
 lpa_status lpa_get_segments(struct lpa_handle *h, uint32_t *begin, uint32_t *end, uint8_t *bucket,
                             uint8_t *variant, size_t count);

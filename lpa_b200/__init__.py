@@ -120,6 +120,7 @@ class Stats(C.Structure):
         ("launches", C.c_uint64),
         ("decode_ms", C.c_double),
         ("iterate_ms", C.c_double),
+        ("count_ms", C.c_double),
     ]
 
 
@@ -157,6 +158,7 @@ def lib():
     _sig(L, "lpa_decode_csr", [P, u64p, u32p])
     _sig(L, "lpa_get_degrees", [P, u32p, C.c_size_t])
     _sig(L, "lpa_set_dispatch", [P, C.c_int, C.c_int])
+    _sig(L, "lpa_set_plan", [P, C.POINTER(C.c_uint8), C.c_size_t])
     _sig(L, "lpa_get_segments", [P, u32p, u32p, u8p, u8p, C.c_size_t])
     _sig(L, "lpa_hg_generate_road", [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_int, C.c_uint64, PP])
     _sig(L, "lpa_hg_generate_rmat", [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
@@ -415,6 +417,10 @@ class Propagator:
         out = np.zeros(MLP_PARAMS, np.float32)
         self._chk(lib().lpa_get_mlp(self._h, _ptr(out, C.c_float), MLP_PARAMS), "lpa_get_mlp")
         return out
+
+    def set_plan(self, plan):
+        a = np.ascontiguousarray(plan, dtype=np.uint8)
+        self._chk(lib().lpa_set_plan(self._h, _ptr(a, C.c_uint8), len(a)), "lpa_set_plan")
 
     def learned_plan(self):
         k = int(self.get_info().num_segments)

@@ -12,8 +12,11 @@
 //      reference (the judge);
 //   2. kExplore iterations on round-robin plans (segment s runs its
 //      ((s + k) mod capable)-th capable variant) -- every step trains the MLP;
-//   3. the MLP's plan runs; if its iteration is slower than the fixed plan's,
-//      the handle reverts to the fixed plan (a revert is counted);
+//   3. the MLP's plan runs, then (when it differs) the same plan with every
+//      capable segment moved to the two-pass kernels -- per-segment costs do
+//      not see a kernel's critical path or launch; the faster of the two is
+//      the learned plan.  If it is slower than the fixed plan, the handle
+//      reverts to the fixed plan (a revert is counted);
 //   4. the chosen plan stays frozen; every kRecheck iterations one iteration
 //      runs the other plan and the faster of the two is kept.
 // Features: degree, compressed bits, interval fraction, residual count (per
@@ -34,7 +37,7 @@ using namespace lpa_mlp;
 namespace {
 
 constexpr int kExplore = 4;
-constexpr int kRecheck = 16;
+constexpr int kRecheck = 64;
 constexpr int kTrainSteps = 64;   // Adam steps after each measured iteration
 constexpr uint32_t kBatch = 4096;  // minibatch (sampled segments)
 constexpr float kLr = 3e-3f;
@@ -173,7 +176,14 @@ void init_params(std::vector<float> &P) {
 
 }  // namespace
 
-enum Phase : int { kPhaseFixed = 0, kPhaseExplore = 1, kPhaseTrial = 2, kPhaseLearned = 3, kPhaseReverted = 4 };
+enum Phase : int {
+  kPhaseFixed = 0,
+  kPhaseExplore = 1,
+  kPhaseTrial = 2,
+  kPhaseLearned = 3,
+  kPhaseReverted = 4,
+  kPhaseTrialMerged = 5
+};
 
 struct Learner {
   float *d_P = nullptr, *d_G = nullptr, *d_M = nullptr, *d_V = nullptr;
@@ -181,6 +191,7 @@ struct Learner {
   float4 *d_feat = nullptr;
   uint8_t *d_cap = nullptr, *d_var = nullptr;
   std::vector<uint8_t> cap, learned;
+  std::vector<uint8_t> merged;  // the MLP's plan with every capable segment on the two-pass kernels
   int phase = kPhaseFixed;
   int explore_k = 0;
   int since_check = 0;
@@ -337,6 +348,9 @@ void lpa_learner_before_iteration(lpa_handle *h) {
     case kPhaseExplore:
       explore_plan(h, L->explore_k, plan);
       break;
+    case kPhaseTrialMerged:
+      plan = L->merged;
+      break;
     case kPhaseTrial:
     case kPhaseLearned:
       plan = (L->since_check >= kRecheck) ? h->fixed : L->learned;
@@ -368,12 +382,29 @@ void lpa_learner_after_iteration(lpa_handle *h) {
       train(h);
       if (++L->explore_k >= kExplore) {
         infer(h);
+        // Per-segment costs do not see a kernel's critical path or its launch:
+        // the plan with the MLP's leftovers moved onto the two-pass kernels
+        // is a second candidate, and the measured iteration time decides.
+        L->merged = L->learned;
+        for (size_t s = 0; s < L->merged.size(); s++)
+          if (variant_capable(LPA_VARIANT_TWO_PASS, h->segs[s], h->opts.cms_threshold))
+            L->merged[s] = LPA_VARIANT_TWO_PASS;
         L->phase = kPhaseTrial;
         L->since_check = 0;
       }
       break;
     case kPhaseTrial:
       L->t_learned = t;
+      if (L->merged != L->learned) {
+        L->phase = kPhaseTrialMerged;
+        break;
+      }
+      [[fallthrough]];
+    case kPhaseTrialMerged:
+      if (L->phase == kPhaseTrialMerged && t < L->t_learned) {
+        L->learned = L->merged;
+        L->t_learned = t;
+      }
       if (L->t_learned > L->t_fixed) {
         L->phase = kPhaseReverted;
         L->reverts++;

@@ -761,7 +761,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
   __syncthreads();
   const Ctx c = resolve(a);
   unsigned long long changed = 0;
-  uint32_t *qctr = a.work + 2 * (a.it_dev ? c.it : 0u);
+  uint32_t *qctr = a.work + 4 * (a.it_dev ? c.it : 0u);
 
   // heavy items: one segment per block (largest first).  The next item is
   // claimed before the current one runs and its bits are prefetched into L2.
@@ -790,7 +790,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
     for (uint32_t p = sg.begin; p < sg.end; p++) heavy_vertex(a, c, sh, stage, tab, s, p, from_scratch, changed);
     if (a.seg_cycles && t == 0)
       atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s),
-                (unsigned long long)((clock64() - t0) * kWarps));
+                (unsigned long long)((clock64() - t0) * kWarps * a.cw_iterate));
   }
 
   // light chunks: a warp claims 4 consecutive chunks at a time, prefetches
@@ -815,7 +815,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
       const long long t0 = clock64();
       light_chunk(a, c, wstage, wslots, wepoch, s, p0, min(sg.end, p0 + 32u), a.seg_var[s], changed);
       if (a.seg_cycles && lane == 0)
-        atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s), (unsigned long long)(clock64() - t0));
+        atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s),
+                  (unsigned long long)((clock64() - t0) * a.cw_iterate));
     }
   }
   flush_changed(c.changed, changed);
@@ -959,7 +960,7 @@ __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs) {
 // segment counts and a 5-step search; the lanes of one position reserve their
 // output range with one atomicAdd on the position's cursor, since the labels
 // of a position may sit in any order.  No block barriers: warps run alone.
-__global__ void __launch_bounds__(kThreads) k_decode_two_pass(IterArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   const DevGraph &g = a.g;
   const Ctx c = resolve(a);
   const uint32_t lane = threadIdx.x & 31u;
@@ -1026,60 +1027,380 @@ __global__ void __launch_bounds__(kThreads) k_decode_two_pass(IterArgs a) {
     uint32_t base = 0;
     if (act && lane == run0 && run_total) base = atomicAdd(a.cursor + p, run_total);
     base = __shfl_sync(kFull, base, run0 & 31u);
+      // residual segments: each lane decodes its own (at most a few hundred bits)
+    uint64_t obase = 0;  // scratch index of this lane's first item
+    bool coop = false;   // an interval segment, expanded by the whole warp below
     if (act) {
       const uint32_t d = g.deg[p];
       const uint32_t off = base + (iincl - items) - run_before;
+      obase = a.arc_off[p] + off;
       if (uint64_t(off) + items > d) {
         bad = true;
+      } else if (items && itv) {
+        coop = true;
       } else if (items) {
-        uint32_t *out = a.scratch + a.arc_off[p] + off;
-        if (!itv) {
-          uint32_t v = 0;
-          for (uint32_t k = 0; k < cnt; k += 4) {
-            uint32_t ids[4];
+        uint32_t *out = a.scratch + obase;
+        uint32_t v = 0;
+        for (uint32_t k = 0; k < cnt; k += 4) {
+          uint32_t ids[4];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
-              ids[u] = node;
-              if (k + u < cnt) {
-                const uint32_t x = r.zeta3(bad);
-                v = (k + u == 0) ? zigzag_first(node, x) : v + x + 1u;
-                ids[u] = v;
-                if (bad || r.pos > end || uint64_t(v) >= g.n) {
-                  bad = true;
-                  ids[u] = node;  // in range; the error word reports the stream
-                }
+          for (int u = 0; u < 4; u++) {
+            ids[u] = node;
+            if (k + u < cnt) {
+              const uint32_t x = r.zeta3(bad);
+              v = (k + u == 0) ? zigzag_first(node, x) : v + x + 1u;
+              ids[u] = v;
+              if (bad || r.pos > end || uint64_t(v) >= g.n) {
+                bad = true;
+                ids[u] = node;  // in range; the error word reports the stream
               }
             }
-            uint32_t lv[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) lv[u] = (k + u < cnt) ? ld_label(c, ids[u]) : 0u;
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-              if (k + u < cnt) out[k + u] = lv[u];
           }
-        } else {
-          r.seek(g.words, q);
-          r.gamma(bad);
-          uint32_t left = 0, w = 0;
-          for (uint32_t k = 0; k < cnt; k++) {
-            const uint32_t l = r.gamma(bad);
-            left = (k == 0) ? zigzag_first(node, l) : left + l + 1u;
-            const uint32_t len = r.gamma(bad) + kMinItv;
-            if (bad || uint64_t(left) + len > g.n || w + len > items) {
-              bad = true;
-              break;
-            }
-            for (uint32_t e = 0; e < len; e++) out[w + e] = ld_label(c, left + e);
-            w += len;
-            left += len;
-          }
+          uint32_t lv[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) lv[u] = (k + u < cnt) ? ld_label(c, ids[u]) : 0u;
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (k + u < cnt) out[k + u] = lv[u];
         }
       }
     }
+    // interval segments: one (left, len) pair per lane per round; the warp
+    // expands the round's intervals together (an interval can hold thousands
+    // of ids), each lane taking every 32nd id of the concatenation
+    if (__any_sync(kFull, coop)) {
+      uint32_t left_todo = 0, nextbase = 0, w = 0;
+      if (coop) {
+        r.seek(g.words, q);
+        left_todo = r.gamma(bad);
+      }
+      // a section's last segment takes the overflow of the one before: < 512 bits, < 256 pairs
+      for (uint32_t round = 0; round < 512u && __any_sync(kFull, coop && left_todo); round++) {
+        uint32_t lo = 0, len = 0;
+        if (coop && left_todo) {
+          const uint32_t l = r.gamma(bad);
+          lo = (left_todo == cnt) ? zigzag_first(node, l) : nextbase + l + 1u;
+          len = r.gamma(bad) + kMinItv;
+          left_todo--;
+          if (bad || uint64_t(lo) + len > g.n || w + len > items) {
+            bad = true;
+            len = 0;
+            left_todo = 0;
+          }
+          nextbase = lo + len;
+        }
+        const uint32_t incl2 = warp_incl_scan(len, lane);
+        const uint32_t tot = __shfl_sync(kFull, incl2, 31);
+        const uint64_t dst = obase + w;  // where this lane's interval goes
+        // 4 ids per lane per step, their loads in flight together
+        for (uint32_t i0 = 0; i0 < tot; i0 += 128) {
+          uint32_t lv[4];
+          uint64_t at[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const uint32_t i = i0 + 32u * u + lane;
+            uint32_t ow = 0;
+#pragma unroll
+            for (uint32_t st = 16; st; st >>= 1) {
+              const uint32_t v = __shfl_sync(kFull, incl2, ow + st - 1);
+              if (v <= i) ow += st;
+            }
+            ow &= 31u;
+            const uint32_t first = __shfl_sync(kFull, incl2 - len, ow);
+            const uint32_t olo = __shfl_sync(kFull, lo, ow);
+            const uint64_t odst = (uint64_t(__shfl_sync(kFull, uint32_t(dst >> 32), ow)) << 32) |
+                                  __shfl_sync(kFull, uint32_t(dst), ow);
+            at[u] = odst + (i - first);
+            lv[u] = i < tot ? ld_label(c, olo + (i - first)) : 0u;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (i0 + 32u * u + lane < tot) a.scratch[at[u]] = lv[u];
+        }
+        w += len;
+      }
+      if (coop && (left_todo || w != items)) bad = true;
+    }
     if (__any_sync(kFull, bad) && lane == 0) set_error(a.err, kErrBadStream);
     if (a.seg_cycles && lane == 0)
-      atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + gd.seg), (unsigned long long)(clock64() - t0));
+      atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + gd.seg),
+                (unsigned long long)((clock64() - t0) * a.cw_decode));
   }
+}
+
+namespace {
+
+// f(ok, label) for this warp's share of src[0..d): 256-label blocks w,
+// w + nw, ... with 8 loads per lane in flight; warp-synchronous.  keep: the
+// labels will be read again soon (keep them in L2).
+template <bool keep, class F>
+__device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ src, uint32_t d, uint32_t w, uint32_t nw,
+                                            F &&f, const uint32_t *__restrict__ labels = nullptr) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t b0 = w * 256u; b0 < d; b0 += nw * 256u) {
+    uint32_t v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const uint32_t k = b0 + 32u * u + lane;
+      v[u] = k < d ? (keep ? __ldcg(src + k) : __ldcs(src + k)) : 0u;
+    }
+    if (labels) {  // src holds ids: gather their labels
+#pragma unroll
+      for (int u = 0; u < 8; u++) v[u] = (b0 + 32u * u + lane < d) ? __ldg(labels + v[u]) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const uint32_t k = b0 + 32u * u;
+      if (k < d) f(k + lane < d, v[u]);
+    }
+  }
+}
+
+// A warp-uniform run of one label: a step whose real labels all equal the
+// run's label only adds to the run's count (two ballots), so a vertex whose
+// neighbours share one label touches its table once per label change, not
+// once per step.  extend() is called by all 32 lanes.
+struct WarpRun {
+  uint32_t lab = kFull, cnt = 0;
+  __device__ __forceinline__ bool extend(bool ok, uint32_t l) {
+    const uint32_t okm = __ballot_sync(kFull, ok);
+    if (__ballot_sync(kFull, ok && l == lab) != okm) return false;
+    cnt += __popc(okm);
+    return true;
+  }
+  // starts a new run at the label of the step's first real lane (the step
+  // itself is counted by the caller)
+  __device__ __forceinline__ void restart(bool ok, uint32_t l) {
+    const uint32_t okm = __ballot_sync(kFull, ok);
+    lab = __shfl_sync(kFull, l, __ffs(okm) - 1);
+    cnt = 0;
+  }
+};
+
+// Exact counts of this warp's share of src[0..d) into et, with a running
+// argmax in best (the count insert() returns is the label's total so far).
+__device__ __forceinline__ void count_exact(const EpochTable &et, const uint32_t *__restrict__ src, uint32_t d,
+                                            uint32_t w, uint32_t nw, uint64_t &best,
+                                            const uint32_t *__restrict__ labels = nullptr) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const auto ins = [&](uint32_t lab, uint32_t c) {
+    const uint64_t cand = pack_best(et.insert(lab, c), lab);
+    best = cand > best ? cand : best;
+  };
+  WarpRun run;
+  warp_stream<false>(src, d, w, nw, [&](bool ok, uint32_t lab) {
+    if (run.extend(ok, lab)) return;
+    if (run.cnt && lane == 0) ins(run.lab, run.cnt);
+    run.restart(ok, lab);
+    const uint32_t c = warp_merge(ok, lab);
+    if (c) ins(lab, c);
+  }, labels);
+  if (run.cnt && lane == 0) ins(run.lab, run.cnt);
+}
+
+// Block-wide maximum of v, returned to every thread.
+__device__ __forceinline__ uint64_t block_max_u64(uint64_t v, uint64_t *red) {
+  v = warp_max_u64(v);
+  if ((threadIdx.x & 31u) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  uint64_t m = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; w++) m = red[w] > m ? red[w] : m;
+  __syncthreads();
+  return m;
+}
+
+}  // namespace
+
+// Two-pass variant, pass 2.  The labels of every compressed two-pass
+// position sit in the scratch, so this kernel mostly streams and counts
+// (positions of the small CSR gather their labels); it holds no staging area
+// and runs four blocks per SM.  Block items (largest first): exact
+// degrees up to kCountBlockMax in a 4096-slot block table, or the sketch;
+// the warps stream disjoint 256-label blocks of the vertex.  Warp items: up
+// to 4 positions of degree <= kCountWarpMax, one vertex at a time in the
+// warp's 512-slot table, or up to 32 positions of degree <= 32 on G-lane
+// groups.  The same shared memory serves the warp tables, the block table
+// (block epochs, disjoint from the warps') and the sketch (cleared before and
+// after use).  Every position's pre-pass cursor is reset here.
+__global__ void __launch_bounds__(kThreads, 4) k_count_two_pass(IterArgs a) {
+  extern __shared__ unsigned long long cslots[];
+  __shared__ uint64_t red[kWarps];
+  __shared__ uint32_t s_item, s_epoch;
+  const DevGraph &g = a.g;
+  const Ctx c = resolve(a);
+  const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+  for (uint32_t i = t; i < kCountBlockSlots; i += kThreads) cslots[i] = 0ull;
+  if (t == 0) s_epoch = kHeavyEpochFirst;
+  __syncthreads();
+  uint32_t *qctr = a.work + 4 * (a.it_dev ? c.it : 0u) + 2;
+  unsigned long long changed = 0;
+
+  for (;;) {
+    if (t == 0) s_item = atomicAdd(qctr, 1u);
+    __syncthreads();
+    const uint32_t i = s_item;
+    __syncthreads();
+    if (i >= a.n_cblock) break;
+    const CountItem it = a.cblock[i];
+    const long long t0 = clock64();
+    const uint32_t p = it.p0;
+    const uint32_t node = g.vertices[p];
+    const uint32_t d = g.deg[p];
+    const uint32_t old = ld_label(c, node);
+    const uint32_t *src = a.scratch + a.arc_off[p];
+    if (t == 0) a.cursor[p] = 0u;
+    uint64_t best = 0;
+    if (it.kind == kCountSketch) {
+      uint32_t *cms = reinterpret_cast<uint32_t *>(cslots);
+      for (uint32_t k = t; k < kCmsDepth * kCmsWidth; k += kThreads) cms[k] = 0u;
+      __syncthreads();
+      const auto add = [&](uint32_t lab, uint32_t w) {
+#pragma unroll
+        for (int r = 0; r < kCmsDepth; r++)
+          atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, lab ^ a.seeds[r]) & (kCmsWidth - 1))], w);
+      };
+      WarpRun run;
+      warp_stream<true>(src, d, warp, kWarps, [&](bool ok, uint32_t lab) {
+        if (run.extend(ok, lab)) return;
+        if (run.cnt && lane == 0) add(run.lab, run.cnt);
+        run.restart(ok, lab);
+        const uint32_t w = warp_merge(ok, lab);
+        if (w) add(lab, w);
+      });
+      if (run.cnt && lane == 0) add(run.lab, run.cnt);
+      __syncthreads();
+      // the estimate depends on the label only: a step whose labels all equal
+      // the label evaluated last adds nothing
+      uint32_t seen = kFull;
+      warp_stream<false>(src, d, warp, kWarps, [&](bool ok, uint32_t lab) {
+        const uint32_t okm = __ballot_sync(kFull, ok);
+        if (__ballot_sync(kFull, ok && lab == seen) == okm) return;
+        seen = __shfl_sync(kFull, lab, __ffs(okm) - 1);
+        if (warp_merge(ok, lab)) {
+          uint32_t est = kFull;
+#pragma unroll
+          for (int r = 0; r < kCmsDepth; r++) {
+            const uint32_t v = cms[r * kCmsWidth + (cm_hash(r, lab ^ a.seeds[r]) & (kCmsWidth - 1))];
+            est = v < est ? v : est;
+          }
+          const uint64_t cand = pack_best(est, lab);
+          best = cand > best ? cand : best;
+        }
+      });
+      best = block_max_u64(best, red);
+      // leave no counter behind that a table could read as one of its slots
+      for (uint32_t k = t; k < kCmsDepth * kCmsWidth; k += kThreads) cms[k] = 0u;
+      __syncthreads();
+    } else {
+      if (t == 0) {
+        if (++s_epoch > 0xFFFFu) s_epoch = 0;  // wrapped: clear below
+      }
+      __syncthreads();
+      if (s_epoch == 0) {
+        for (uint32_t k = t; k < kCountBlockSlots; k += kThreads) cslots[k] = 0ull;
+        __syncthreads();
+        if (t == 0) s_epoch = kHeavyEpochFirst;
+        __syncthreads();
+      }
+      const EpochTable et{cslots, min(next_pow2(2 * d), kCountBlockSlots), s_epoch};
+      count_exact(et, src, d, warp, kWarps, best);
+      best = block_max_u64(best, red);
+    }
+    if (t == 0) {
+      const uint32_t nl = d ? best_label(best) : old;
+      c.lab_out[node] = nl;
+      changed += (nl != old);
+      if (a.seg_changed && nl != old) atomicAdd(a.seg_changed + it.seg, 1u);
+      if (a.seg_cycles)
+        atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + it.seg),
+                  (unsigned long long)((clock64() - t0) * kWarps * a.cw_count));
+    }
+  }
+
+  unsigned long long *wslots = cslots + warp * kCountWarpSlots;
+  uint32_t wepoch = 0;
+  for (;;) {
+    uint32_t i0 = 0;
+    if (lane == 0) i0 = atomicAdd(qctr + 1, 2u);
+    i0 = __shfl_sync(kFull, i0, 0);
+    if (i0 >= a.n_cwarp) break;
+    for (uint32_t q = i0; q < i0 + 2u && q < a.n_cwarp; q++) {
+      const CountItem it = a.cwarp[q];
+      const long long t0 = clock64();
+      uint32_t my_changed = 0;
+      if (it.kind == kCountGroups) {
+        const uint32_t p = it.p0 + lane;
+        const bool valid = lane < it.np;
+        const uint32_t node = valid ? g.vertices[p] : 0u;
+        const uint32_t d = valid ? g.deg[p] : 0u;
+        const uint32_t old = valid ? ld_label(c, node) : 0u;
+        // compressed positions: labels in the scratch; the small CSR: ids
+        const bool ids = it.p0 >= g.n_c;
+        const uint64_t ao = !valid ? 0ull : (ids ? uint64_t(g.small_off[p - g.n_c]) : a.arc_off[p]);
+        if (valid && !ids) a.cursor[p] = 0u;
+        const uint32_t dmax = __reduce_max_sync(kFull, d);
+        const uint32_t G = next_pow2(dmax);
+        const uint32_t per = 32 / G;
+        const uint32_t gl = lane / G, k = lane % G;
+        const uint32_t gm = (G == 32) ? kFull : (((1u << G) - 1u) << (gl * G));
+        for (uint32_t v0 = 0; v0 < it.np; v0 += per) {
+          const uint32_t vi = v0 + gl;
+          const bool vin = vi < it.np;
+          const uint32_t srcl = vin ? vi : 0u;
+          const uint32_t dv = __shfl_sync(kFull, d, srcl);
+          const uint32_t nodev = __shfl_sync(kFull, node, srcl);
+          const uint32_t oldv = __shfl_sync(kFull, old, srcl);
+          const uint64_t aov = (uint64_t(__shfl_sync(kFull, uint32_t(ao >> 32), srcl)) << 32) |
+                               __shfl_sync(kFull, uint32_t(ao), srcl);
+          const bool ok = vin && k < dv;
+          const uint32_t lab = !ok ? kFull : (ids ? ld_label(c, __ldg(g.small_nbr + aov + k)) : __ldcs(a.scratch + aov + k));
+          const uint32_t cnt = group_counts(ok, lab, gm, gl);
+          const uint32_t maxc = __reduce_max_sync(gm, cnt);
+          const uint32_t bestl = __reduce_min_sync(gm, (ok && cnt == maxc) ? lab : kFull);
+          if (vin && k == 0) {
+            const uint32_t nl = dv ? bestl : oldv;
+            c.lab_out[nodev] = nl;
+            my_changed += (nl != oldv);
+          }
+        }
+      } else {
+        for (uint32_t j = 0; j < it.np; j++) {
+          const uint32_t p = it.p0 + j;
+          const uint32_t node = g.vertices[p];
+          const uint32_t d = g.deg[p];
+          const uint32_t old = ld_label(c, node);
+          const bool ids = p >= g.n_c;
+          if (lane == 0 && !ids) a.cursor[p] = 0u;
+          if (++wepoch >= kLightEpochs) {
+            for (uint32_t k = lane; k < kCountWarpSlots; k += 32) wslots[k] = 0ull;
+            __syncwarp();
+            wepoch = 1;
+          }
+          const EpochTable et{wslots, min(next_pow2(2 * d), kCountWarpSlots), wepoch};
+          uint64_t bp = 0;
+          if (ids) count_exact(et, g.small_nbr + g.small_off[p - g.n_c], d, 0, 1, bp, c.lab_in);
+          else count_exact(et, a.scratch + a.arc_off[p], d, 0, 1, bp);
+          bp = warp_max_u64(bp);
+          if (lane == 0) {
+            const uint32_t nl = d ? best_label(bp) : old;
+            c.lab_out[node] = nl;
+            my_changed += (nl != old);
+          }
+          __syncwarp();
+        }
+      }
+      changed += my_changed;
+      const uint32_t sc = __reduce_add_sync(kFull, my_changed);
+      if (lane == 0) {
+        if (a.seg_changed && sc) atomicAdd(a.seg_changed + it.seg, sc);
+        if (a.seg_cycles)
+          atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + it.seg),
+                    (unsigned long long)((clock64() - t0) * a.cw_count));
+      }
+    }
+  }
+  flush_changed(c.changed, changed);
 }
 
 __global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err) {

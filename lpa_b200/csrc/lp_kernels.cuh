@@ -49,6 +49,24 @@ struct DecodeGroup {
   uint32_t p0, j0, nlanes, seg;
 };
 
+// Work of the two-pass count pass (k_count_two_pass): positions p0 ..
+// p0 + np - 1, all of one kind, whose labels the pre-pass wrote to the
+// scratch.  seg is the plan segment the cycles are booked to.
+enum CountKind : uint32_t {
+  kCountGroups = 0,  // np <= 32 positions of degree <= 32: G-lane groups, several vertices per round
+  kCountWarp = 1,    // np <= 4 positions of degree <= kCountWarpMax: warp per vertex, 512-slot table
+  kCountBlock = 2,   // one position, degree <= kCountBlockMax: block per vertex, 4096-slot table
+  kCountSketch = 3,  // one position at or above the sketch threshold: block per vertex
+};
+struct CountItem {
+  uint32_t p0, np, seg, kind;
+};
+constexpr uint32_t kCountWarpSlots = 512;
+constexpr uint32_t kCountWarpMax = 255;
+constexpr uint32_t kCountBlockSlots = kWarps * kCountWarpSlots;  // the warps' tables together
+constexpr uint32_t kCountBlockMax = 2047;
+constexpr uint32_t kCountSmemBytes = kCountBlockSlots * 8;        // 32 KB
+
 struct IterArgs {
   DevGraph g;
   uint32_t *labs0, *labs1;      // the two label buffers
@@ -66,8 +84,16 @@ struct IterArgs {
   const DecodeGroup *groups;    // two-pass pre-pass work: 32 segments per group
   uint32_t n_groups;
   const uint4 *pidx;            // per compressed position: {ibase - offset, rbase - offset, nseg_i, nseg_r}
+  const CountItem *cblock;      // count-pass block items (largest first), then warp items
+  uint32_t n_cblock;
+  const CountItem *cwarp;
+  uint32_t n_cwarp;
   uint32_t *cursor;             // per compressed position: labels written by the pre-pass (pass 2 resets)
   long long *seg_cycles;        // per-segment device cycles (nullptr: off)
+  // weights of one warp-cycle of k_iterate / k_decode_two_pass /
+  // k_count_two_pass in seg_cycles: 64 / (the kernel's resident warps per
+  // SM), so a booked cycle is a cycle of 1/64 of an SM whichever kernel spent it
+  uint32_t cw_iterate, cw_decode, cw_count;
   uint32_t *seg_changed;        // per-segment changed counts (nullptr: off)
   uint32_t cms_thr;             // 0: no sketch
   uint32_t seeds[kCmsDepth];
@@ -121,6 +147,8 @@ __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs);
 
 __global__ void k_iterate(IterArgs a);
 __global__ void k_decode_two_pass(IterArgs a);
+// Two-pass variant, pass 2: counts the labels the pre-pass wrote.
+__global__ void k_count_two_pass(IterArgs a);
 
 struct DecodeArgs {
   DevGraph g;

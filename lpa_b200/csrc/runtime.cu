@@ -212,12 +212,48 @@ static void upload_lists(lpa_handle *h) {
   // compressed region are decoded by the pre-pass.
   std::vector<WorkItem> heavy, light;
   std::vector<DecodeGroup> groups;
+  std::vector<CountItem> cblock, cwarp;
+  const uint32_t cms = h->opts.cms_threshold;
   for (size_t s = 0; s < h->segs.size(); s++) {
     const int v = h->variant[s];
     const SegInfo &si = h->segs[s];
     const bool tp = v == LPA_VARIANT_TWO_PASS;
     const bool block = v == LPA_VARIANT_BLOCK || (tp && !variant_capable(LPA_VARIANT_WARP, si, h->opts.cms_threshold));
-    if (block) {
+    bool counted = false;  // two-pass positions counted by k_count_two_pass
+    if (tp) {
+      counted = true;
+      for (uint32_t p = si.begin; p < si.end; p++) {
+        const uint32_t d = h->h_deg[p];
+        if ((cms == 0 || d < cms) && d > kCountBlockMax) counted = false;  // exact above the block table
+        // the small CSR is counted by warp items only (block items read the scratch)
+        if (si.region == 1 && ((cms != 0 && d >= cms) || d > kCountWarpMax)) counted = false;
+      }
+    }
+    if (counted) {
+      // runs of consecutive positions of one kind
+      uint32_t p = si.begin;
+      while (p < si.end) {
+        const uint32_t d = h->h_deg[p];
+        if (cms != 0 && d >= cms) {
+          cblock.push_back(CountItem{p, 1, uint32_t(s), kCountSketch});
+          p++;
+        } else if (d > kCountWarpMax) {
+          cblock.push_back(CountItem{p, 1, uint32_t(s), kCountBlock});
+          p++;
+        } else {
+          const bool small = d <= 32;
+          const uint32_t cap = small ? 32u : 4u;
+          uint32_t q = p + 1;
+          while (q < si.end && q - p < cap) {
+            const uint32_t dq = h->h_deg[q];
+            if ((cms != 0 && dq >= cms) || dq > kCountWarpMax || (dq <= 32) != small) break;
+            q++;
+          }
+          cwarp.push_back(CountItem{p, q - p, uint32_t(s), small ? kCountGroups : kCountWarp});
+          p = q;
+        }
+      }
+    } else if (block) {
       heavy.push_back(make_item(h, uint32_t(s), si.begin, si.end, tp));
     } else {
       const uint32_t chunks = (si.end - si.begin + 31) / 32;
@@ -253,6 +289,14 @@ static void upload_lists(lpa_handle *h) {
   std::stable_sort(heavy.begin(), heavy.end(), [&](const WorkItem &a, const WorkItem &b) {
     return h->segs[a.tag].arcs > h->segs[b.tag].arcs;
   });
+  std::stable_sort(cblock.begin(), cblock.end(),
+                   [&](const CountItem &a, const CountItem &b) { return h->h_deg[a.p0] > h->h_deg[b.p0]; });
+  h->n_cblock = uint32_t(cblock.size());
+  h->n_cwarp = uint32_t(cwarp.size());
+  std::vector<CountItem> citems;
+  citems.reserve(cblock.size() + cwarp.size());
+  citems.insert(citems.end(), cblock.begin(), cblock.end());
+  citems.insert(citems.end(), cwarp.begin(), cwarp.end());
   h->n_heavy = uint32_t(heavy.size());
   h->n_light = uint32_t(light.size());
   h->n_groups = uint32_t(groups.size());
@@ -272,6 +316,8 @@ static void upload_lists(lpa_handle *h) {
   };
   regrow(h->d_items, h->items_cap, all.size(), "work items");
   regrow(h->d_groups, h->groups_cap, groups.size(), "decode groups");
+  regrow(h->d_citems, h->citems_cap, citems.size(), "count items");
+  h2d(h, h->d_citems, citems.data(), citems.size(), "upload count items");
   h2d(h, h->d_items, all.data(), all.size(), "upload work items");
   h2d(h, h->d_groups, groups.data(), groups.size(), "upload decode groups");
   h2d(h, h->d_seg_var, h->variant.data(), h->variant.size(), "upload variants");
@@ -410,9 +456,16 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.n_light = h->n_light;
   a.groups = h->d_groups;
   a.n_groups = h->n_groups;
+  a.cblock = h->d_citems;
+  a.n_cblock = h->n_cblock;
+  a.cwarp = h->d_citems + h->n_cblock;
+  a.n_cwarp = h->n_cwarp;
   a.pidx = h->d_pidx;
   a.cursor = h->d_cursor;
   a.seg_cycles = (h->opts.record_timings >= 2 || h->collect_cycles) ? h->d_seg_cycles : nullptr;
+  a.cw_iterate = h->cw_iterate;
+  a.cw_decode = h->cw_decode;
+  a.cw_count = h->cw_count;
   a.seg_changed = h->learner ? h->d_seg_changed : nullptr;
   a.cms_thr = h->opts.cms_threshold;
   for (int r = 0; r < kCmsDepth; r++) a.seeds[r] = h->seeds[r];
@@ -436,9 +489,16 @@ static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32
     h->launches++;
   }
   if (timed) cudaEventRecord(h->ev[1], h->stream);
-  k_iterate<<<h->grid, kThreads, kSmemBytes, h->stream>>>(a);
-  h->launches++;
+  if (h->n_cblock + h->n_cwarp) {
+    k_count_two_pass<<<h->grid_count, kThreads, kCountSmemBytes, h->stream>>>(a);
+    h->launches++;
+  }
   if (timed) cudaEventRecord(h->ev[2], h->stream);
+  if (h->n_heavy + h->n_light) {
+    k_iterate<<<h->grid, kThreads, kSmemBytes, h->stream>>>(a);
+    h->launches++;
+  }
+  if (timed) cudaEventRecord(h->ev[3], h->stream);
   h->cur ^= 1;
 }
 
@@ -454,8 +514,9 @@ static void collect_times(lpa_handle *h) {
   };
   for (int v = 0; v < 4; v++) h->variant_ms[v] = 0;
   h->decode_ms = ms(0, 1);
-  h->iterate_ms = ms(1, 2);
-  h->last_iter_ms = ms(0, 2);
+  h->count_ms = ms(1, 2);
+  h->iterate_ms = ms(2, 3);
+  h->last_iter_ms = ms(0, 3);
 }
 
 // ------------------------------------------------------------------ C ABI --
@@ -539,6 +600,16 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ, k_iterate, kThreads, kSmemBytes), "occupancy");
     h->occ = std::max(1, h->occ);
     h->grid = h->num_sms * h->occ;
+    int occ_count = 1;
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_count, k_count_two_pass, kThreads, kCountSmemBytes),
+          "occupancy");
+    h->grid_count = h->num_sms * std::max(1, occ_count);
+    int occ_decode = 1;
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_decode, k_decode_two_pass, kThreads, 0), "occupancy");
+    const auto weight = [](int blocks) { return uint32_t(std::max(1, 64 / (std::max(1, blocks) * kWarps))); };
+    h->cw_iterate = weight(h->occ);
+    h->cw_count = weight(occ_count);
+    h->cw_decode = weight(occ_decode);
 
     h->n = n;
     h->n_c = n_c;
@@ -564,8 +635,8 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     h->d_lab[1] = dalloc<uint32_t>(h, n, "labels");
     h->changed_slots = kMaxRunSlots;
     h->d_changed = dalloc<unsigned long long>(h, h->changed_slots, "changed counters");
-    h->d_work = dalloc<uint32_t>(h, 2 * size_t(h->changed_slots), "work counters");
-    check(h, cudaMemsetAsync(h->d_work, 0, 2 * size_t(h->changed_slots) * sizeof(uint32_t), h->stream),
+    h->d_work = dalloc<uint32_t>(h, 4 * size_t(h->changed_slots), "work counters");
+    check(h, cudaMemsetAsync(h->d_work, 0, 4 * size_t(h->changed_slots) * sizeof(uint32_t), h->stream),
           "clear work counters");
     check(h, cudaMemsetAsync(h->d_changed, 0, h->changed_slots * sizeof(unsigned long long), h->stream),
           "clear counters");
@@ -674,7 +745,7 @@ lpa_status lpa_iterate(lpa_handle *h, uint64_t *changed_out) {
     lpa_learner_before_iteration(h);
     unsigned long long *slot = h->d_changed;
     check(h, cudaMemsetAsync(slot, 0, sizeof(unsigned long long), h->stream), "clear counter");
-    check(h, cudaMemsetAsync(h->d_work, 0, 2 * sizeof(uint32_t), h->stream), "clear work counters");
+    check(h, cudaMemsetAsync(h->d_work, 0, 4 * sizeof(uint32_t), h->stream), "clear work counters");
     enqueue_iteration(h, slot, h->d_work);
     check(h, cudaGetLastError(), "iteration launch");
     check(h, cudaMemcpyAsync(h->h_pinned, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream),
@@ -746,6 +817,7 @@ lpa_status lpa_get_stats(lpa_handle *h, lpa_stats *st) {
   st->launches = h->launches;
   st->decode_ms = h->decode_ms;
   st->iterate_ms = h->iterate_ms;
+  st->count_ms = h->count_ms;
   for (int v = 0; v < 4; v++) st->variant_ms[v] = h->variant_ms[v];
   for (size_t s = 0; s < h->segs.size(); s++) {
     st->variant_segments[h->variant[s]]++;
@@ -814,6 +886,23 @@ lpa_status lpa_set_dispatch(lpa_handle *h, int dispatch, int force_variant) {
     lpa_learner_reset(h);
     apply_dispatch(h, dispatch == LPA_DISPATCH_FORCE ? LPA_DISPATCH_FORCE : LPA_DISPATCH_FIXED, force_variant);
     check(h, cudaStreamSynchronize(h->stream), "dispatch");
+  } catch (const Fail &f) {
+    return guard(h, f);
+  }
+  return LPA_OK;
+}
+
+lpa_status lpa_set_plan(lpa_handle *h, const uint8_t *variant, size_t count) {
+  if (!h || !variant || count != h->segs.size()) return LPA_ERR_INVALID_ARG;
+  for (size_t s = 0; s < count; s++)
+    if (variant[s] > 3 || !variant_capable(variant[s], h->segs[s], h->opts.cms_threshold)) return LPA_ERR_INVALID_ARG;
+  try {
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    h->opts.dispatch = LPA_DISPATCH_FORCE;
+    lpa_learner_reset(h);
+    h->variant.assign(variant, variant + count);
+    lpa_rt_apply_variants(h);
+    check(h, cudaStreamSynchronize(h->stream), "plan");
   } catch (const Fail &f) {
     return guard(h, f);
   }

@@ -81,6 +81,11 @@ struct lpa_handle {
   uint4 *d_pidx = nullptr;                   // per compressed position: section starts and segment counts
   std::vector<uint32_t> h_nseg;              // per compressed position: interval + residual segments
   uint32_t *d_cursor = nullptr;              // per compressed position: pre-pass output cursor
+  lpa_dev::CountItem *d_citems = nullptr;    // count-pass block items, then warp items
+  uint32_t n_cblock = 0, n_cwarp = 0;
+  size_t citems_cap = 0;
+  int grid_count = 0;                        // count-pass kernel
+  uint32_t cw_iterate = 1, cw_decode = 1, cw_count = 1;  // seg_cycles weights (64 / resident warps per SM)
   std::vector<uint64_t> h_offsets;        // host copies for the prefetch ranges
   std::vector<uint32_t> h_small_off;
   std::vector<uint64_t> h_arc_off;
@@ -106,9 +111,9 @@ struct lpa_handle {
   std::vector<uint64_t> history;
   double last_iter_ms = 0;
   double variant_ms[4] = {0, 0, 0, 0};
-  double decode_ms = 0, iterate_ms = 0;
+  double decode_ms = 0, iterate_ms = 0, count_ms = 0;
   bool collect_cycles = false;  // per-segment cycles for the cost model
-  cudaEvent_t ev[4] = {};  // two-pass decode start/end, iteration start/end
+  cudaEvent_t ev[4] = {};  // iteration start, after the pre-pass, after the count pass, iteration end
   bool events_ready = false;
   uint64_t device_bytes = 0;
   std::vector<void *> allocations;
