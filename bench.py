@@ -490,7 +490,7 @@ def main():
                          "learned_over_fixed": (fixed_ms / total_ms) if args.dispatch == "learned" else None,
                          "learner": learned_info},
             "cpu_baseline": cb,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * arr["n"],
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * arr["n"],
                     "d2h_bytes_per_step": 4 * arr["n"] + 8},
             "gpu_launches": int(st1.launches - st0.launches),
             "clocks": clk,

@@ -961,9 +961,11 @@ __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs) {
 // output range with one atomicAdd on the position's cursor, since the labels
 // of a position may sit in any order.  No block barriers: warps run alone.
 __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
+  __shared__ uint32_t stage[kWarps * kDecodeWindow];
+  __shared__ uint8_t owner[kWarps * kDecodeWindow];
   const DevGraph &g = a.g;
   const Ctx c = resolve(a);
-  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < a.n_groups; gi += nw) {
     const long long t0 = clock64();
@@ -1027,43 +1029,61 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
     uint32_t base = 0;
     if (act && lane == run0 && run_total) base = atomicAdd(a.cursor + p, run_total);
     base = __shfl_sync(kFull, base, run0 & 31u);
-      // residual segments: each lane decodes its own (at most a few hundred bits)
+      // residual segments, in windows of kDecodeWindow items of the group:
+    // each lane decodes its own segment's ids into the warp's staging area
+    // (its lane number beside each), then the warp gathers the window's
+    // labels with 8 loads per lane in flight and stores them, consecutive
+    // ids of a position to consecutive addresses
     uint64_t obase = 0;  // scratch index of this lane's first item
     bool coop = false;   // an interval segment, expanded by the whole warp below
+    uint32_t ritems = 0;
     if (act) {
       const uint32_t d = g.deg[p];
       const uint32_t off = base + (iincl - items) - run_before;
       obase = a.arc_off[p] + off;
-      if (uint64_t(off) + items > d) {
-        bad = true;
-      } else if (items && itv) {
-        coop = true;
-      } else if (items) {
-        uint32_t *out = a.scratch + obase;
-        uint32_t v = 0;
-        for (uint32_t k = 0; k < cnt; k += 4) {
-          uint32_t ids[4];
+      if (uint64_t(off) + items > d) bad = true;
+      else if (items && itv) coop = true;
+      else ritems = items;
+    }
+    const uint32_t rincl = warp_incl_scan(ritems, lane);
+    const uint32_t rexcl = rincl - ritems;
+    const uint32_t rtot = __shfl_sync(kFull, rincl, 31);
+    uint32_t *wst = stage + warp * kDecodeWindow;
+    uint8_t *wown = owner + warp * kDecodeWindow;
+    uint32_t done = 0, v = 0;
+    for (uint32_t w0 = 0; w0 < rtot; w0 += kDecodeWindow) {
+      const uint32_t w1 = min(w0 + kDecodeWindow, rtot);
+      while (done < ritems && rexcl + done < w1) {
+        const uint32_t x = r.zeta3(bad);
+        v = (done == 0) ? zigzag_first(node, x) : v + x + 1u;
+        uint32_t id = v;
+        if (bad || r.pos > end || uint64_t(v) >= g.n) {
+          bad = true;
+          id = node;  // in range; the error word reports the stream
+        }
+        wst[rexcl + done - w0] = id;
+        wown[rexcl + done - w0] = uint8_t(lane);
+        done++;
+      }
+      __syncwarp();
+      for (uint32_t f0 = w0; f0 < w1; f0 += 256) {
+        uint32_t lv[8];
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            ids[u] = node;
-            if (k + u < cnt) {
-              const uint32_t x = r.zeta3(bad);
-              v = (k + u == 0) ? zigzag_first(node, x) : v + x + 1u;
-              ids[u] = v;
-              if (bad || r.pos > end || uint64_t(v) >= g.n) {
-                bad = true;
-                ids[u] = node;  // in range; the error word reports the stream
-              }
-            }
-          }
-          uint32_t lv[4];
+        for (int u = 0; u < 8; u++) {
+          const uint32_t f = f0 + 32u * u + lane;
+          lv[u] = f < w1 ? ld_label(c, wst[f - w0]) : 0u;
+        }
 #pragma unroll
-          for (int u = 0; u < 4; u++) lv[u] = (k + u < cnt) ? ld_label(c, ids[u]) : 0u;
-#pragma unroll
-          for (int u = 0; u < 4; u++)
-            if (k + u < cnt) out[k + u] = lv[u];
+        for (int u = 0; u < 8; u++) {
+          const uint32_t f = f0 + 32u * u + lane;
+          const uint32_t ol = f < w1 ? wown[f - w0] : 0u;
+          const uint64_t ob = (uint64_t(__shfl_sync(kFull, uint32_t(obase >> 32), ol)) << 32) |
+                              __shfl_sync(kFull, uint32_t(obase), ol);
+          const uint32_t ox = __shfl_sync(kFull, rexcl, ol);
+          if (f < w1) a.scratch[ob + (f - ox)] = lv[u];
         }
       }
+      __syncwarp();
     }
     // interval segments: one (left, len) pair per lane per round; the warp
     // expands the round's intervals together (an interval can hold thousands
@@ -1339,6 +1359,31 @@ __global__ void __launch_bounds__(kThreads, 4) k_count_two_pass(IterArgs a) {
         const bool ids = it.p0 >= g.n_c;
         const uint64_t ao = !valid ? 0ull : (ids ? uint64_t(g.small_off[p - g.n_c]) : a.arc_off[p]);
         if (valid && !ids) a.cursor[p] = 0u;
+        // the positions are consecutive, so their neighbours are one range:
+        // stage all its labels in the warp's table memory first (8 loads per
+        // lane in flight), then count from shared memory
+        const uint32_t incl = warp_incl_scan(d, lane);
+        const uint32_t excl = incl - d;
+        const uint32_t total = __shfl_sync(kFull, incl, 31);  // <= 32 * 32
+        const uint64_t ao0 = (uint64_t(__shfl_sync(kFull, uint32_t(ao >> 32), 0)) << 32) |
+                             __shfl_sync(kFull, uint32_t(ao), 0);
+        uint32_t *wstage = reinterpret_cast<uint32_t *>(wslots);
+        for (uint32_t k0 = 0; k0 < total; k0 += 256) {
+          uint32_t v[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            const uint32_t kk = k0 + 32u * u + lane;
+            v[u] = kk >= total ? 0u : (ids ? __ldg(g.small_nbr + ao0 + kk) : __ldcs(a.scratch + ao0 + kk));
+          }
+          if (ids) {
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = (k0 + 32u * u + lane < total) ? ld_label(c, v[u]) : 0u;
+          }
+#pragma unroll
+          for (int u = 0; u < 8; u++)
+            if (k0 + 32u * u + lane < total) wstage[k0 + 32u * u + lane] = v[u];
+        }
+        __syncwarp();
         const uint32_t dmax = __reduce_max_sync(kFull, d);
         const uint32_t G = next_pow2(dmax);
         const uint32_t per = 32 / G;
@@ -1351,25 +1396,32 @@ __global__ void __launch_bounds__(kThreads, 4) k_count_two_pass(IterArgs a) {
           const uint32_t dv = __shfl_sync(kFull, d, srcl);
           const uint32_t nodev = __shfl_sync(kFull, node, srcl);
           const uint32_t oldv = __shfl_sync(kFull, old, srcl);
-          const uint64_t aov = (uint64_t(__shfl_sync(kFull, uint32_t(ao >> 32), srcl)) << 32) |
-                               __shfl_sync(kFull, uint32_t(ao), srcl);
+          const uint32_t ev = __shfl_sync(kFull, excl, srcl);
           const bool ok = vin && k < dv;
-          const uint32_t lab = !ok ? kFull : (ids ? ld_label(c, __ldg(g.small_nbr + aov + k)) : __ldcs(a.scratch + aov + k));
+          const uint32_t lab = ok ? wstage[ev + k] : kFull;
           const uint32_t cnt = group_counts(ok, lab, gm, gl);
           const uint32_t maxc = __reduce_max_sync(gm, cnt);
           const uint32_t bestl = __reduce_min_sync(gm, (ok && cnt == maxc) ? lab : kFull);
-          if (vin && k == 0) {
-            const uint32_t nl = dv ? bestl : oldv;
-            c.lab_out[nodev] = nl;
-            my_changed += (nl != oldv);
+          if (vin && k == 0 && dv) {  // an isolated vertex keeps its label in both buffers
+            c.lab_out[nodev] = bestl;
+            my_changed += (bestl != oldv);
           }
         }
+        __syncwarp();
+        // the staged labels must not read as table slots later
+        for (uint32_t k2 = lane; k2 < (total + 1) / 2; k2 += 32) wslots[k2] = 0ull;
+        __syncwarp();
       } else {
+        // every vertex's metadata in one round of loads (lane j: vertex j)
+        const bool vj = lane < it.np;
+        const uint32_t nodej = vj ? g.vertices[it.p0 + lane] : 0u;
+        const uint32_t dj = vj ? g.deg[it.p0 + lane] : 0u;
+        const uint32_t oldj = vj ? ld_label(c, nodej) : 0u;
         for (uint32_t j = 0; j < it.np; j++) {
           const uint32_t p = it.p0 + j;
-          const uint32_t node = g.vertices[p];
-          const uint32_t d = g.deg[p];
-          const uint32_t old = ld_label(c, node);
+          const uint32_t node = __shfl_sync(kFull, nodej, j);
+          const uint32_t d = __shfl_sync(kFull, dj, j);
+          const uint32_t old = __shfl_sync(kFull, oldj, j);
           const bool ids = p >= g.n_c;
           if (lane == 0 && !ids) a.cursor[p] = 0u;
           if (++wepoch >= kLightEpochs) {

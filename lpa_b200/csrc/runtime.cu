@@ -214,6 +214,8 @@ static void upload_lists(lpa_handle *h) {
   std::vector<DecodeGroup> groups;
   std::vector<CountItem> cblock, cwarp;
   const uint32_t cms = h->opts.cms_threshold;
+  // per position: 1 + the plan segment of a counted position of degree <= 32
+  std::vector<uint32_t> gmark(h->n, 0);
   for (size_t s = 0; s < h->segs.size(); s++) {
     const int v = h->variant[s];
     const SegInfo &si = h->segs[s];
@@ -240,16 +242,16 @@ static void upload_lists(lpa_handle *h) {
         } else if (d > kCountWarpMax) {
           cblock.push_back(CountItem{p, 1, uint32_t(s), kCountBlock});
           p++;
+        } else if (d <= 32) {
+          gmark[p++] = uint32_t(s) + 1;  // group items are formed below, across segments
         } else {
-          const bool small = d <= 32;
-          const uint32_t cap = small ? 32u : 4u;
           uint32_t q = p + 1;
-          while (q < si.end && q - p < cap) {
+          while (q < si.end && q - p < 4) {
             const uint32_t dq = h->h_deg[q];
-            if ((cms != 0 && dq >= cms) || dq > kCountWarpMax || (dq <= 32) != small) break;
+            if ((cms != 0 && dq >= cms) || dq > kCountWarpMax || dq <= 32) break;
             q++;
           }
-          cwarp.push_back(CountItem{p, q - p, uint32_t(s), small ? kCountGroups : kCountWarp});
+          cwarp.push_back(CountItem{p, q - p, uint32_t(s), kCountWarp});
           p = q;
         }
       }
@@ -289,6 +291,25 @@ static void upload_lists(lpa_handle *h) {
   std::stable_sort(heavy.begin(), heavy.end(), [&](const WorkItem &a, const WorkItem &b) {
     return h->segs[a.tag].arcs > h->segs[b.tag].arcs;
   });
+  // group items: up to 32 consecutive positions of one region, each either
+  // marked above or without neighbours (isolated vertices are in no segment
+  // and cut segments short; an item runs across them, since they add no
+  // arcs and keep their label).  Cycles are booked to the first position's
+  // segment.
+  for (uint64_t p = 0; p < h->n;) {
+    if (!gmark[p]) {
+      p++;
+      continue;
+    }
+    const bool reg = p >= h->n_c;
+    uint64_t q = p, last = p;
+    while (q < h->n && q - p < 32 && (q >= h->n_c) == reg && (gmark[q] || h->h_deg[q] == 0)) {
+      if (gmark[q]) last = q;
+      q++;
+    }
+    cwarp.push_back(CountItem{uint32_t(p), uint32_t(last + 1 - p), gmark[p] - 1, kCountGroups});
+    p = last + 1;
+  }
   std::stable_sort(cblock.begin(), cblock.end(),
                    [&](const CountItem &a, const CountItem &b) { return h->h_deg[a.p0] > h->h_deg[b.p0]; });
   h->n_cblock = uint32_t(cblock.size());
@@ -726,7 +747,7 @@ lpa_status lpa_set_labels(lpa_handle *h, const uint32_t *host, size_t n) {
     check(h, cudaSetDevice(h->device), "cudaSetDevice");
     // both buffers: vertices without neighbours are never rewritten
     check(h, cudaMemcpyAsync(h->d_lab[0], host, n * 4, cudaMemcpyHostToDevice, h->stream), "set labels");
-    check(h, cudaMemcpyAsync(h->d_lab[1], host, n * 4, cudaMemcpyHostToDevice, h->stream), "set labels");
+    check(h, cudaMemcpyAsync(h->d_lab[1], h->d_lab[0], n * 4, cudaMemcpyDeviceToDevice, h->stream), "set labels");
     check(h, cudaStreamSynchronize(h->stream), "set labels");
     h->cur = 0;
     h->iterations = 0;
