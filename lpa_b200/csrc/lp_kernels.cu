@@ -1384,27 +1384,40 @@ __global__ void __launch_bounds__(kThreads, 4) k_count_two_pass(IterArgs a) {
             if (k0 + 32u * u + lane < total) wstage[k0 + 32u * u + lane] = v[u];
         }
         __syncwarp();
-        const uint32_t dmax = __reduce_max_sync(kFull, d);
-        const uint32_t G = next_pow2(dmax);
-        const uint32_t per = 32 / G;
-        const uint32_t gl = lane / G, k = lane % G;
-        const uint32_t gm = (G == 32) ? kFull : (((1u << G) - 1u) << (gl * G));
-        for (uint32_t v0 = 0; v0 < it.np; v0 += per) {
-          const uint32_t vi = v0 + gl;
-          const bool vin = vi < it.np;
-          const uint32_t srcl = vin ? vi : 0u;
-          const uint32_t dv = __shfl_sync(kFull, d, srcl);
-          const uint32_t nodev = __shfl_sync(kFull, node, srcl);
-          const uint32_t oldv = __shfl_sync(kFull, old, srcl);
-          const uint32_t ev = __shfl_sync(kFull, excl, srcl);
-          const bool ok = vin && k < dv;
-          const uint32_t lab = ok ? wstage[ev + k] : kFull;
-          const uint32_t cnt = group_counts(ok, lab, gm, gl);
-          const uint32_t maxc = __reduce_max_sync(gm, cnt);
-          const uint32_t bestl = __reduce_min_sync(gm, (ok && cnt == maxc) ? lab : kFull);
-          if (vin && k == 0 && dv) {  // an isolated vertex keeps its label in both buffers
-            c.lab_out[nodev] = bestl;
-            my_changed += (bestl != oldv);
+        // a vertex whose labels are all equal takes that label: lane v checks
+        // its own vertex; only the others are counted below
+        bool mixed = false;
+        const uint32_t first = (lane < it.np && d) ? wstage[excl] : 0u;
+        for (uint32_t j = 1; j < d; j++) mixed |= wstage[excl + j] != first;
+        if (lane < it.np && d && !mixed) {  // an isolated vertex keeps its label in both buffers
+          c.lab_out[node] = first;
+          my_changed += (first != old);
+        }
+        const uint32_t rest = __ballot_sync(kFull, mixed);
+        if (rest) {
+          // G-lane groups over the mixed vertices, 32 / G of them a round
+          const uint32_t nrest = __popc(rest);
+          const uint32_t dmax = __reduce_max_sync(kFull, mixed ? d : 0u);
+          const uint32_t G = next_pow2(dmax);
+          const uint32_t per = 32 / G;
+          const uint32_t gl = lane / G, k = lane % G;
+          const uint32_t gm = (G == 32) ? kFull : (((1u << G) - 1u) << (gl * G));
+          for (uint32_t v0 = 0; v0 < nrest; v0 += per) {
+            const bool vin = v0 + gl < nrest;
+            const uint32_t srcl = vin ? __fns(rest, 0, v0 + gl + 1) : 0u;
+            const uint32_t dv = __shfl_sync(kFull, d, srcl);
+            const uint32_t nodev = __shfl_sync(kFull, node, srcl);
+            const uint32_t oldv = __shfl_sync(kFull, old, srcl);
+            const uint32_t ev = __shfl_sync(kFull, excl, srcl);
+            const bool ok = vin && k < dv;
+            const uint32_t lab = ok ? wstage[ev + k] : kFull;
+            const uint32_t cnt = group_counts(ok, lab, gm, gl);
+            const uint32_t maxc = __reduce_max_sync(gm, cnt);
+            const uint32_t bestl = __reduce_min_sync(gm, (ok && cnt == maxc) ? lab : kFull);
+            if (vin && k == 0) {
+              c.lab_out[nodev] = bestl;
+              my_changed += (bestl != oldv);
+            }
           }
         }
         __syncwarp();
