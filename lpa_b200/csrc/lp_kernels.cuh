@@ -63,7 +63,7 @@ struct CountItem {
   uint32_t p0, np, seg, kind;
 };
 constexpr uint32_t kCountWarpSlots = 512;
-constexpr uint32_t kCountWarpMax = 255;
+constexpr uint32_t kCountWarpMax = kCountWarpSlots - 1;  // tables fill up to load 1 (triangular probing)
 constexpr uint32_t kCountBlockSlots = kWarps * kCountWarpSlots;  // the warps' tables together
 constexpr uint32_t kCountBlockMax = 2047;
 constexpr uint32_t kCountSmemBytes = kCountBlockSlots * 8;        // 32 KB
