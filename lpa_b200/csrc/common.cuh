@@ -449,6 +449,13 @@ __device__ __forceinline__ uint32_t group_counts(bool ok, uint32_t lab, uint32_t
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// The GPU's nanosecond clock (the same for every SM).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Bulk prefetch of [p, p + bytes) into L2 (cp.async.bulk.prefetch, sm_90+):
 // one instruction per range, rounded out to 16-byte boundaries, split into
 // pieces below 1 MiB.

@@ -19,6 +19,8 @@
 //      reverts to the fixed plan (a revert is counted);
 //   4. the chosen plan stays frozen; every kRecheck iterations one iteration
 //      runs the other plan and the faster of the two is kept.
+// Times compared in 3 and 4 are the iteration's kernel busy time on the GPU
+// clock (IterArgs::ktime), not host-visible wall time.
 // Features: degree, compressed bits, interval fraction, residual count (per
 // vertex of the segment), iteration index and the segment's change rate in
 // the previous iteration.
@@ -361,6 +363,8 @@ void lpa_learner_before_iteration(lpa_handle *h) {
   set_plan(h, plan);
   h->collect_cycles = true;
   cudaMemsetAsync(h->d_seg_cycles, 0, std::max<size_t>(1, h->segs.size()) * sizeof(long long), h->stream);
+  cudaMemsetAsync(h->d_ktime, 0xFF, 3 * sizeof(unsigned long long), h->stream);  // starts: none yet
+  cudaMemsetAsync(h->d_ktime + 3, 0, 3 * sizeof(unsigned long long), h->stream);  // ends
   std::swap(h->d_seg_changed, h->d_seg_changed_prev);
   cudaMemsetAsync(h->d_seg_changed, 0, std::max<size_t>(1, h->segs.size()) * sizeof(uint32_t), h->stream);
 }
@@ -369,7 +373,20 @@ void lpa_learner_after_iteration(lpa_handle *h) {
   h->collect_cycles = false;
   Learner *L = h->learner;
   if (!L || h->opts.dispatch != LPA_DISPATCH_LEARNED) return;
-  const double t = h->last_iter_ms;
+  // The judge's clock: the time the iteration's kernels were busy on the GPU
+  // (the sum of their spans on the GPU clock).  Unlike the events around the
+  // iteration, it leaves out host-side gaps between launches, which a tool
+  // such as a profiler can stretch by orders of magnitude.
+  double t = h->last_iter_ms;
+  unsigned long long span[6];
+  if (cudaMemcpy(span, h->d_ktime, sizeof(span), cudaMemcpyDeviceToHost) == cudaSuccess) {
+    double busy = 0;
+    for (int k = 0; k < 3; k++)
+      if (span[3 + k] > span[k]) busy += double(span[3 + k] - span[k]) * 1e-6;
+    if (busy > 0) t = busy;
+  } else {
+    cudaGetLastError();
+  }
   const bool fixed_now = h->variant == h->fixed;
   switch (L->phase) {
     case kPhaseFixed:

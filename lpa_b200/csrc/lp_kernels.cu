@@ -750,6 +750,15 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, un
 
 }  // namespace
 
+// Widens the kernel's busy span in a.ktime by this warp's start or end.
+__device__ __forceinline__ void busy_mark(const IterArgs &a, int kernel, bool end) {
+  if (a.ktime && (threadIdx.x & 31u) == 0) {
+    const unsigned long long t = global_ns();
+    if (end) atomicMax(a.ktime + 3 + kernel, t);
+    else atomicMin(a.ktime + kernel, t);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
   extern __shared__ uint32_t smem[];
   __shared__ BlockSh sh;
@@ -760,6 +769,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
   if (t == 0) sh.hepoch = kHeavyEpochFirst;
   __syncthreads();
   const Ctx c = resolve(a);
+  busy_mark(a, 2, false);
   unsigned long long changed = 0;
   uint32_t *qctr = a.work + 4 * (a.it_dev ? c.it : 0u);
 
@@ -819,6 +829,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
                   (unsigned long long)((clock64() - t0) * a.cw_iterate));
     }
   }
+  busy_mark(a, 2, true);
   flush_changed(c.changed, changed);
 }
 
@@ -890,6 +901,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchArgs b) {
       ia.n_groups = 0;
       ia.pidx = nullptr;
       ia.cursor = nullptr;
+      ia.ktime = nullptr;
       ia.gtab = b.gtab;
       ia.gtab_slots = b.gtab_slots;
     }
@@ -965,6 +977,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   __shared__ uint8_t owner[kWarps * kDecodeWindow];
   const DevGraph &g = a.g;
   const Ctx c = resolve(a);
+  busy_mark(a, 0, false);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < a.n_groups; gi += nw) {
@@ -1146,6 +1159,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
       atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + gd.seg),
                 (unsigned long long)((clock64() - t0) * a.cw_decode));
   }
+  busy_mark(a, 0, true);
 }
 
 namespace {
@@ -1249,6 +1263,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_count_two_pass(IterArgs a) {
   __shared__ uint32_t s_item, s_epoch;
   const DevGraph &g = a.g;
   const Ctx c = resolve(a);
+  busy_mark(a, 1, false);
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   for (uint32_t i = t; i < kCountBlockSlots; i += kThreads) cslots[i] = 0ull;
   if (t == 0) s_epoch = kHeavyEpochFirst;
@@ -1465,6 +1480,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_count_two_pass(IterArgs a) {
       }
     }
   }
+  busy_mark(a, 1, true);
   flush_changed(c.changed, changed);
 }
 

@@ -95,6 +95,10 @@ struct IterArgs {
   // k_count_two_pass in seg_cycles: 64 / (the kernel's resident warps per
   // SM), so a booked cycle is a cycle of 1/64 of an SM whichever kernel spent it
   uint32_t cw_iterate, cw_decode, cw_count;
+  // nullptr, or the busy span of each kernel of the iteration on the GPU's
+  // clock (ns): ktime[k] = earliest warp start, ktime[3 + k] = latest warp end,
+  // k = 0 k_decode_two_pass, 1 k_count_two_pass, 2 k_iterate
+  unsigned long long *ktime;
   uint32_t *seg_changed;        // per-segment changed counts (nullptr: off)
   uint32_t cms_thr;             // 0: no sketch
   uint32_t seeds[kCmsDepth];

@@ -436,6 +436,7 @@ static void build_plan(lpa_handle *h) {
   h2d(h, h->d_segs, ds.data(), ds.size(), "upload segments");
   check(h, cudaStreamSynchronize(h->stream), "upload segments");
   h->d_seg_cycles = dalloc<long long>(h, h->segs.size(), "segment cycles");
+  h->d_ktime = dalloc<unsigned long long>(h, 6, "kernel busy spans");
   check(h, cudaMemsetAsync(h->d_seg_cycles, 0, std::max<size_t>(1, h->segs.size()) * sizeof(long long), h->stream),
         "clear cycles");
 
@@ -487,6 +488,7 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.cw_iterate = h->cw_iterate;
   a.cw_decode = h->cw_decode;
   a.cw_count = h->cw_count;
+  a.ktime = h->collect_cycles ? h->d_ktime : nullptr;
   a.seg_changed = h->learner ? h->d_seg_changed : nullptr;
   a.cms_thr = h->opts.cms_threshold;
   for (int r = 0; r < kCmsDepth; r++) a.seeds[r] = h->seeds[r];

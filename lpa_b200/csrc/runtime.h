@@ -103,6 +103,7 @@ struct lpa_handle {
   uint32_t gtab_slots = 0;
   int gtab_blocks = 0;
   long long *d_seg_cycles = nullptr;
+  unsigned long long *d_ktime = nullptr;  // busy span of each kernel of a learning iteration (IterArgs::ktime)
 
   // stats
   uint64_t iterations = 0;

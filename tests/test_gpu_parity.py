@@ -183,3 +183,26 @@ def test_dispatch_switch_keeps_labels_identical():
             p.set_dispatch(L.Dispatch.FORCE, v)
             p.iterate()
             assert np.array_equal(p.labels(), hist[it])
+
+
+@pytest.mark.parametrize("case", ["rmat_t16", "stress"])
+def test_explicit_plan_mixes_variants_exactly(case):
+    """lpa_set_plan: a random mix of the variants each segment can run gives
+    the oracle's labels after every iteration; a plan with a variant a segment
+    cannot run is refused and leaves the plan in place."""
+    g, ref = _load(case)
+    with L.Propagator(g, cms_threshold=8) as p:
+        _, _, bucket, fixed = p.segments()
+        rng = np.random.default_rng(7)
+        # the fixed plan's variant, or the block or two-pass variant (both run
+        # every segment)
+        choice = rng.integers(0, 3, size=len(fixed))
+        plan = np.where(choice == 0, fixed, np.where(choice == 1, int(L.Variant.TWO_PASS), int(L.Variant.BLOCK)))
+        p.set_plan(plan.astype(np.uint8))
+        _check_iterations(p, ref["row"], ref["clm"], 4, 8)
+        if (bucket >= 1).any():  # several vertices per warp: not for sketch or degree > 32
+            bad = np.full(len(fixed), int(L.Variant.PACKED), np.uint8)
+            with pytest.raises(L.LpaError) as e:
+                p.set_plan(bad)
+            assert e.value.status == L.Status.INVALID_ARG
+            assert np.array_equal(p.segments()[3], plan)
