@@ -2,8 +2,8 @@
 """Benchmark: one synchronous label-propagation iteration over a CGR graph.
 
 Metric: decoded arcs x iterations per second (every stored arc is decoded and
-its label counted once per iteration), with the roofline of the dominant
-kernel against the measured HBM copy bandwidth.
+its label counted once per iteration), with the roofline of one iteration
+(its kernels together) against the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rmat-s24]
     python bench.py --impl reference ...   # the CPU path (oracle port), same metric
@@ -274,7 +274,7 @@ def measured_peak_gbs():
 
 
 def traffic_summary(workload: str):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    """DRAM bytes per iteration (its kernels together) from the committed ncu summaries."""
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
         try:
