@@ -1249,7 +1249,7 @@ __device__ __forceinline__ uint64_t block_max_u64(uint64_t v, uint64_t *red) {
 // Two-pass variant, pass 2.  The labels of every compressed two-pass
 // position sit in the scratch, so this kernel mostly streams and counts
 // (positions of the small CSR gather their labels); it holds no staging area
-// and runs four blocks per SM.  Block items (largest first): exact
+// and runs five blocks per SM (48 registers).  Block items (largest first): exact
 // degrees up to kCountBlockMax in a 4096-slot block table, or the sketch;
 // the warps stream disjoint 256-label blocks of the vertex.  Warp items: up
 // to 4 positions of degree <= kCountWarpMax, one vertex at a time in the
@@ -1257,7 +1257,7 @@ __device__ __forceinline__ uint64_t block_max_u64(uint64_t v, uint64_t *red) {
 // groups.  The same shared memory serves the warp tables, the block table
 // (block epochs, disjoint from the warps') and the sketch (cleared before and
 // after use).  Every position's pre-pass cursor is reset here.
-__global__ void __launch_bounds__(kThreads, 4) k_count_two_pass(IterArgs a) {
+__global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
   extern __shared__ unsigned long long cslots[];
   __shared__ uint64_t red[kWarps];
   __shared__ uint32_t s_item, s_epoch;

@@ -92,8 +92,8 @@ struct IterArgs {
   uint32_t *cursor;             // per compressed position: labels written by the pre-pass (pass 2 resets)
   long long *seg_cycles;        // per-segment device cycles (nullptr: off)
   // weights of one warp-cycle of k_iterate / k_decode_two_pass /
-  // k_count_two_pass in seg_cycles: 64 / (the kernel's resident warps per
-  // SM), so a booked cycle is a cycle of 1/64 of an SM whichever kernel spent it
+  // k_count_two_pass in seg_cycles: 960 / (the kernel's resident warps per
+  // SM), so a booked unit is the same share of an SM whichever kernel spent it
   uint32_t cw_iterate, cw_decode, cw_count;
   // nullptr, or the busy span of each kernel of the iteration on the GPU's
   // clock (ns): ktime[k] = earliest warp start, ktime[3 + k] = latest warp end,

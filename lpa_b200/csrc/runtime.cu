@@ -629,7 +629,8 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     h->grid_count = h->num_sms * std::max(1, occ_count);
     int occ_decode = 1;
     check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_decode, k_decode_two_pass, kThreads, 0), "occupancy");
-    const auto weight = [](int blocks) { return uint32_t(std::max(1, 64 / (std::max(1, blocks) * kWarps))); };
+    // 960 is divisible by every resident warp count these kernels reach (16..64 in steps of 8)
+    const auto weight = [](int blocks) { return uint32_t(std::max(1, 960 / (std::max(1, blocks) * kWarps))); };
     h->cw_iterate = weight(h->occ);
     h->cw_count = weight(occ_count);
     h->cw_decode = weight(occ_decode);

@@ -38,7 +38,7 @@ def test_two_replicas_share_graph_and_max_time():
     pytest.importorskip("torch")
     world = 2
     name = f"test_{uuid.uuid4().hex[:8]}"
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_worker, args=(world, _free_port(), name, out), nprocs=world, join=True)
         res = dict(out)
