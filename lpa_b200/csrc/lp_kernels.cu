@@ -1260,7 +1260,8 @@ __device__ __forceinline__ uint64_t block_max_u64(uint64_t v, uint64_t *red) {
 __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
   extern __shared__ unsigned long long cslots[];
   __shared__ uint64_t red[kWarps];
-  __shared__ uint32_t s_item, s_epoch;
+  __shared__ uint32_t s_has, s_epoch;
+  __shared__ BlockItem s_bi;
   const DevGraph &g = a.g;
   const Ctx c = resolve(a);
   busy_mark(a, 1, false);
@@ -1271,20 +1272,41 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
   uint32_t *qctr = a.work + 4 * (a.it_dev ? c.it : 0u) + 2;
   unsigned long long changed = 0;
 
+  // Block items, claimed ahead: while the block works on item k, thread 0
+  // holds item k + 1 (loaded) and the claim of item k + 2, so neither the
+  // queue atomic nor the item load sits on an item's critical path.  An item
+  // carries its position's degree, scratch offset and vertex id, so the
+  // block streams labels at once.
+  BlockItem nxt{};
+  bool has_nxt = false;
+  uint32_t claim = 0;
+  if (t == 0) {
+    const uint32_t c0 = atomicAdd(qctr, 1u), c1 = atomicAdd(qctr, 1u);
+    s_has = c0 < a.n_cblock;
+    if (s_has) s_bi = a.cblock[c0];
+    has_nxt = c1 < a.n_cblock;
+    if (has_nxt) nxt = a.cblock[c1];
+    claim = atomicAdd(qctr, 1u);
+    if (++s_epoch > 0xFFFFu) s_epoch = 0;
+  }
   for (;;) {
-    if (t == 0) s_item = atomicAdd(qctr, 1u);
     __syncthreads();
-    const uint32_t i = s_item;
-    __syncthreads();
-    if (i >= a.n_cblock) break;
-    const CountItem it = a.cblock[i];
+    if (!s_has) break;
+    const BlockItem it = s_bi;
+    if (s_epoch == 0) {  // the block epochs wrapped: clear the table once
+      for (uint32_t k = t; k < kCountBlockSlots; k += kThreads) cslots[k] = 0ull;
+      __syncthreads();
+      if (t == 0) s_epoch = kHeavyEpochFirst;
+    }
+    __syncthreads();  // every thread holds the item before thread 0 moves on
     const long long t0 = clock64();
-    const uint32_t p = it.p0;
-    const uint32_t node = g.vertices[p];
-    const uint32_t d = g.deg[p];
-    const uint32_t old = ld_label(c, node);
-    const uint32_t *src = a.scratch + a.arc_off[p];
-    if (t == 0) a.cursor[p] = 0u;
+    const uint32_t d = it.d;
+    const uint32_t *src = a.scratch + it.ao;
+    uint32_t old = 0;
+    if (t == 0) {
+      a.cursor[it.p] = 0u;
+      old = ld_label(c, it.node);  // needed at the end only
+    }
     uint64_t best = 0;
     if (it.kind == kCountSketch) {
       uint32_t *cms = reinterpret_cast<uint32_t *>(cslots);
@@ -1326,30 +1348,26 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
       best = block_max_u64(best, red);
       // leave no counter behind that a table could read as one of its slots
       for (uint32_t k = t; k < kCmsDepth * kCmsWidth; k += kThreads) cms[k] = 0u;
-      __syncthreads();
     } else {
-      if (t == 0) {
-        if (++s_epoch > 0xFFFFu) s_epoch = 0;  // wrapped: clear below
-      }
-      __syncthreads();
-      if (s_epoch == 0) {
-        for (uint32_t k = t; k < kCountBlockSlots; k += kThreads) cslots[k] = 0ull;
-        __syncthreads();
-        if (t == 0) s_epoch = kHeavyEpochFirst;
-        __syncthreads();
-      }
       const EpochTable et{cslots, min(next_pow2(2 * d), kCountBlockSlots), s_epoch};
       count_exact(et, src, d, warp, kWarps, best);
       best = block_max_u64(best, red);
     }
     if (t == 0) {
       const uint32_t nl = d ? best_label(best) : old;
-      c.lab_out[node] = nl;
+      c.lab_out[it.node] = nl;
       changed += (nl != old);
       if (a.seg_changed && nl != old) atomicAdd(a.seg_changed + it.seg, 1u);
       if (a.seg_cycles)
         atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + it.seg),
                   (unsigned long long)((clock64() - t0) * kWarps * a.cw_count));
+      // advance the pipeline (the block reads s_bi after the loop-top barrier)
+      s_has = has_nxt;
+      s_bi = nxt;
+      has_nxt = claim < a.n_cblock;
+      if (has_nxt) nxt = a.cblock[claim];
+      claim = atomicAdd(qctr, 1u);
+      if (++s_epoch > 0xFFFFu) s_epoch = 0;
     }
   }
 

@@ -62,6 +62,12 @@ enum CountKind : uint32_t {
 struct CountItem {
   uint32_t p0, np, seg, kind;
 };
+// A block item of the count pass, with everything its block needs up front.
+struct BlockItem {
+  uint64_t ao;              // scratch index of the position's labels (arc offset)
+  uint32_t p, d, node;      // position, degree, vertex id
+  uint32_t seg, kind, pad;  // plan segment (cycles), kCountBlock or kCountSketch
+};
 constexpr uint32_t kCountWarpSlots = 512;
 constexpr uint32_t kCountWarpMax = kCountWarpSlots - 1;  // tables fill up to load 1 (triangular probing)
 constexpr uint32_t kCountBlockSlots = kWarps * kCountWarpSlots;  // the warps' tables together
@@ -85,7 +91,7 @@ struct IterArgs {
   const DecodeGroup *groups;    // two-pass pre-pass work: 32 segments per group
   uint32_t n_groups;
   const uint4 *pidx;            // per compressed position: {ibase - offset, rbase - offset, nseg_i, nseg_r}
-  const CountItem *cblock;      // count-pass block items (largest first), then warp items
+  const BlockItem *cblock;      // count-pass block items (largest first)
   uint32_t n_cblock;
   const CountItem *cwarp;
   uint32_t n_cwarp;

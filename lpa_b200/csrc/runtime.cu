@@ -212,7 +212,8 @@ static void upload_lists(lpa_handle *h) {
   // compressed region are decoded by the pre-pass.
   std::vector<WorkItem> heavy, light;
   std::vector<DecodeGroup> groups;
-  std::vector<CountItem> cblock, cwarp;
+  std::vector<BlockItem> cblock;
+  std::vector<CountItem> cwarp;
   const uint32_t cms = h->opts.cms_threshold;
   // per position: 1 + the plan segment of a counted position of degree <= 32
   std::vector<uint32_t> gmark(h->n, 0);
@@ -237,10 +238,10 @@ static void upload_lists(lpa_handle *h) {
       while (p < si.end) {
         const uint32_t d = h->h_deg[p];
         if (cms != 0 && d >= cms) {
-          cblock.push_back(CountItem{p, 1, uint32_t(s), kCountSketch});
+          cblock.push_back(BlockItem{h->h_arc_off[p], p, d, h->h_vertices[p], uint32_t(s), kCountSketch, 0});
           p++;
         } else if (d > kCountWarpMax) {
-          cblock.push_back(CountItem{p, 1, uint32_t(s), kCountBlock});
+          cblock.push_back(BlockItem{h->h_arc_off[p], p, d, h->h_vertices[p], uint32_t(s), kCountBlock, 0});
           p++;
         } else if (d <= 32) {
           gmark[p++] = uint32_t(s) + 1;  // group items are formed below, across segments
@@ -310,14 +311,10 @@ static void upload_lists(lpa_handle *h) {
     cwarp.push_back(CountItem{uint32_t(p), uint32_t(last + 1 - p), gmark[p] - 1, kCountGroups});
     p = last + 1;
   }
-  std::stable_sort(cblock.begin(), cblock.end(),
-                   [&](const CountItem &a, const CountItem &b) { return h->h_deg[a.p0] > h->h_deg[b.p0]; });
+  std::stable_sort(cblock.begin(), cblock.end(), [](const BlockItem &a, const BlockItem &b) { return a.d > b.d; });
   h->n_cblock = uint32_t(cblock.size());
   h->n_cwarp = uint32_t(cwarp.size());
-  std::vector<CountItem> citems;
-  citems.reserve(cblock.size() + cwarp.size());
-  citems.insert(citems.end(), cblock.begin(), cblock.end());
-  citems.insert(citems.end(), cwarp.begin(), cwarp.end());
+  const std::vector<CountItem> &citems = cwarp;
   h->n_heavy = uint32_t(heavy.size());
   h->n_light = uint32_t(light.size());
   h->n_groups = uint32_t(groups.size());
@@ -338,6 +335,8 @@ static void upload_lists(lpa_handle *h) {
   regrow(h->d_items, h->items_cap, all.size(), "work items");
   regrow(h->d_groups, h->groups_cap, groups.size(), "decode groups");
   regrow(h->d_citems, h->citems_cap, citems.size(), "count items");
+  regrow(h->d_cblock, h->cblock_cap, cblock.size(), "count block items");
+  h2d(h, h->d_cblock, cblock.data(), cblock.size(), "upload count block items");
   h2d(h, h->d_citems, citems.data(), citems.size(), "upload count items");
   h2d(h, h->d_items, all.data(), all.size(), "upload work items");
   h2d(h, h->d_groups, groups.data(), groups.size(), "upload decode groups");
@@ -478,9 +477,9 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.n_light = h->n_light;
   a.groups = h->d_groups;
   a.n_groups = h->n_groups;
-  a.cblock = h->d_citems;
+  a.cblock = h->d_cblock;
   a.n_cblock = h->n_cblock;
-  a.cwarp = h->d_citems + h->n_cblock;
+  a.cwarp = h->d_citems;
   a.n_cwarp = h->n_cwarp;
   a.pidx = h->d_pidx;
   a.cursor = h->d_cursor;
@@ -673,6 +672,7 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     h->h_offsets.assign(g->offsets, g->offsets + (n_c ? n_c + 1 : 0));
     if (n_c == 0) h->h_offsets.assign(1, 0);
     if (n > n_c) h->h_small_off.assign(g->small_offset, g->small_offset + (n - n_c + 1));
+    h->h_vertices.assign(g->vertices, g->vertices + n_c);
     build_plan(h);
     // per-segment stream bits for the cost model's features
     for (auto &s : h->segs)

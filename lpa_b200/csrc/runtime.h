@@ -81,7 +81,10 @@ struct lpa_handle {
   uint4 *d_pidx = nullptr;                   // per compressed position: section starts and segment counts
   std::vector<uint32_t> h_nseg;              // per compressed position: interval + residual segments
   uint32_t *d_cursor = nullptr;              // per compressed position: pre-pass output cursor
-  lpa_dev::CountItem *d_citems = nullptr;    // count-pass block items, then warp items
+  lpa_dev::CountItem *d_citems = nullptr;    // count-pass warp items
+  lpa_dev::BlockItem *d_cblock = nullptr;    // count-pass block items
+  size_t cblock_cap = 0;
+  std::vector<uint32_t> h_vertices;          // vertex id of every compressed position
   uint32_t n_cblock = 0, n_cwarp = 0;
   size_t citems_cap = 0;
   int grid_count = 0;                        // count-pass kernel
