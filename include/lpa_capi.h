@@ -166,6 +166,27 @@ lpa_status lpa_set_dispatch(struct lpa_handle *h, int dispatch, int force_varian
  * No counterpart in the reference, which hard-codes its degree buckets
  * (baselines/novaplus/novaplus_propogator.cuh:219-220). */
 lpa_status lpa_set_plan(struct lpa_handle *h, const uint8_t *variant, size_t count);
+
+/* Work shapes of the two-pass count pass: the autotuner's knobs.  No
+ * counterpart in the reference, whose shapes are compile-time constants. */
+typedef struct lpa_tune {
+  uint32_t group_positions;  /* positions (degree <= 32) per several-vertices warp item, 1..32; default 32 */
+  uint32_t warp_positions;   /* vertices per one-vertex-at-a-time warp item, 1..32; default 4 */
+  uint32_t warp_max_degree;  /* largest degree one warp counts (32..511); a block counts larger; default 511 */
+  uint32_t warp_claim;       /* warp items a warp claims from the queue at once, 1..8; default 2 */
+} lpa_tune;
+lpa_status lpa_get_tune(struct lpa_handle *h, lpa_tune *out);
+/* Installs the knobs (out of range: LPA_ERR_INVALID_ARG) and rebuilds the work lists. */
+lpa_status lpa_set_tune(struct lpa_handle *h, const lpa_tune *t);
+/* Autotuner: searches the knobs one at a time (coordinate descent, two
+ * sweeps) for the current plan.  Every candidate runs `repeats` iterations
+ * (default 2 when <= 0), each from the same label state, and is judged by the
+ * iteration's kernel busy time on the GPU clock; the labels and the iteration
+ * count are as before the call.  With cache_path, a result found there for
+ * this GPU, graph, sketch threshold and plan is installed without a search,
+ * and a new result is appended.  The best knobs are installed and returned in
+ * out (may be NULL). */
+lpa_status lpa_autotune(struct lpa_handle *h, const char *cache_path, int repeats, lpa_tune *out);
 /* Per-segment view of the plan: begin/end positions, bucket, variant. */
 lpa_status lpa_get_segments(struct lpa_handle *h, uint32_t *begin, uint32_t *end, uint8_t *bucket,
                             uint8_t *variant, size_t count);

@@ -64,6 +64,19 @@ class LpaError(RuntimeError):
         super().__init__(msg)
 
 
+class Tune(C.Structure):
+    """Work shapes of the two-pass count pass (lpa_tune)."""
+    _fields_ = [
+        ("group_positions", C.c_uint32),
+        ("warp_positions", C.c_uint32),
+        ("warp_max_degree", C.c_uint32),
+        ("warp_claim", C.c_uint32),
+    ]
+
+    def as_tuple(self):
+        return (self.group_positions, self.warp_positions, self.warp_max_degree, self.warp_claim)
+
+
 class GraphDesc(C.Structure):
     _fields_ = [
         ("num_vertices", C.c_uint64),
@@ -159,6 +172,9 @@ def lib():
     _sig(L, "lpa_get_degrees", [P, u32p, C.c_size_t])
     _sig(L, "lpa_set_dispatch", [P, C.c_int, C.c_int])
     _sig(L, "lpa_set_plan", [P, C.POINTER(C.c_uint8), C.c_size_t])
+    _sig(L, "lpa_get_tune", [P, C.POINTER(Tune)])
+    _sig(L, "lpa_set_tune", [P, C.POINTER(Tune)])
+    _sig(L, "lpa_autotune", [P, C.c_char_p, C.c_int, C.POINTER(Tune)])
     _sig(L, "lpa_get_segments", [P, u32p, u32p, u8p, u8p, C.c_size_t])
     _sig(L, "lpa_hg_generate_road", [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_int, C.c_uint64, PP])
     _sig(L, "lpa_hg_generate_rmat", [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
@@ -421,6 +437,21 @@ class Propagator:
     def set_plan(self, plan):
         a = np.ascontiguousarray(plan, dtype=np.uint8)
         self._chk(lib().lpa_set_plan(self._h, _ptr(a, C.c_uint8), len(a)), "lpa_set_plan")
+
+    def get_tune(self) -> Tune:
+        t = Tune()
+        self._chk(lib().lpa_get_tune(self._h, C.byref(t)), "lpa_get_tune")
+        return t
+
+    def set_tune(self, group_positions, warp_positions, warp_max_degree, warp_claim):
+        t = Tune(group_positions, warp_positions, warp_max_degree, warp_claim)
+        self._chk(lib().lpa_set_tune(self._h, C.byref(t)), "lpa_set_tune")
+
+    def autotune(self, cache_path=None, repeats=2) -> Tune:
+        t = Tune()
+        path = None if cache_path is None else str(cache_path).encode()
+        self._chk(lib().lpa_autotune(self._h, path, int(repeats), C.byref(t)), "lpa_autotune")
+        return t
 
     def learned_plan(self):
         k = int(self.get_info().num_segments)

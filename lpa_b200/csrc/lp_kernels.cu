@@ -1252,7 +1252,7 @@ __device__ __forceinline__ uint64_t block_max_u64(uint64_t v, uint64_t *red) {
 // and runs five blocks per SM (48 registers).  Block items (largest first): exact
 // degrees up to kCountBlockMax in a 4096-slot block table, or the sketch;
 // the warps stream disjoint 256-label blocks of the vertex.  Warp items: up
-// to 4 positions of degree <= kCountWarpMax, one vertex at a time in the
+// to 4 (tunable) positions of degree <= kCountWarpMax, one vertex at a time in the
 // warp's 512-slot table, or up to 32 positions of degree <= 32 on G-lane
 // groups.  The same shared memory serves the warp tables, the block table
 // (block epochs, disjoint from the warps') and the sketch (cleared before and
@@ -1375,10 +1375,11 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
   uint32_t wepoch = 0;
   for (;;) {
     uint32_t i0 = 0;
-    if (lane == 0) i0 = atomicAdd(qctr + 1, 2u);
+    const uint32_t claim = a.warp_claim ? a.warp_claim : 2u;
+    if (lane == 0) i0 = atomicAdd(qctr + 1, claim);
     i0 = __shfl_sync(kFull, i0, 0);
     if (i0 >= a.n_cwarp) break;
-    for (uint32_t q = i0; q < i0 + 2u && q < a.n_cwarp; q++) {
+    for (uint32_t q = i0; q < i0 + claim && q < a.n_cwarp; q++) {
       const CountItem it = a.cwarp[q];
       const long long t0 = clock64();
       uint32_t my_changed = 0;

@@ -95,6 +95,7 @@ struct IterArgs {
   uint32_t n_cblock;
   const CountItem *cwarp;
   uint32_t n_cwarp;
+  uint32_t warp_claim;          // warp items a warp of the count pass claims at once
   uint32_t *cursor;             // per compressed position: labels written by the pre-pass (pass 2 resets)
   long long *seg_cycles;        // per-segment device cycles (nullptr: off)
   // weights of one warp-cycle of k_iterate / k_decode_two_pass /

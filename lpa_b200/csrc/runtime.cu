@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <fstream>
+#include <sstream>
 #include <cstring>
 #include <new>
 #include <string>
@@ -215,6 +217,7 @@ static void upload_lists(lpa_handle *h) {
   std::vector<BlockItem> cblock;
   std::vector<CountItem> cwarp;
   const uint32_t cms = h->opts.cms_threshold;
+  const uint32_t wmax = h->tune.warp_max_degree;  // above: a block item
   // per position: 1 + the plan segment of a counted position of degree <= 32
   std::vector<uint32_t> gmark(h->n, 0);
   for (size_t s = 0; s < h->segs.size(); s++) {
@@ -229,7 +232,7 @@ static void upload_lists(lpa_handle *h) {
         const uint32_t d = h->h_deg[p];
         if ((cms == 0 || d < cms) && d > kCountBlockMax) counted = false;  // exact above the block table
         // the small CSR is counted by warp items only (block items read the scratch)
-        if (si.region == 1 && ((cms != 0 && d >= cms) || d > kCountWarpMax)) counted = false;
+        if (si.region == 1 && ((cms != 0 && d >= cms) || d > wmax)) counted = false;
       }
     }
     if (counted) {
@@ -240,16 +243,16 @@ static void upload_lists(lpa_handle *h) {
         if (cms != 0 && d >= cms) {
           cblock.push_back(BlockItem{h->h_arc_off[p], p, d, h->h_vertices[p], uint32_t(s), kCountSketch, 0});
           p++;
-        } else if (d > kCountWarpMax) {
+        } else if (d > wmax) {
           cblock.push_back(BlockItem{h->h_arc_off[p], p, d, h->h_vertices[p], uint32_t(s), kCountBlock, 0});
           p++;
         } else if (d <= 32) {
           gmark[p++] = uint32_t(s) + 1;  // group items are formed below, across segments
         } else {
           uint32_t q = p + 1;
-          while (q < si.end && q - p < 4) {
+          while (q < si.end && q - p < h->tune.warp_positions) {
             const uint32_t dq = h->h_deg[q];
-            if ((cms != 0 && dq >= cms) || dq > kCountWarpMax || dq <= 32) break;
+            if ((cms != 0 && dq >= cms) || dq > wmax || dq <= 32) break;
             q++;
           }
           cwarp.push_back(CountItem{p, q - p, uint32_t(s), kCountWarp});
@@ -304,7 +307,7 @@ static void upload_lists(lpa_handle *h) {
     }
     const bool reg = p >= h->n_c;
     uint64_t q = p, last = p;
-    while (q < h->n && q - p < 32 && (q >= h->n_c) == reg && (gmark[q] || h->h_deg[q] == 0)) {
+    while (q < h->n && q - p < h->tune.group_positions && (q >= h->n_c) == reg && (gmark[q] || h->h_deg[q] == 0)) {
       if (gmark[q]) last = q;
       q++;
     }
@@ -481,13 +484,14 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.n_cblock = h->n_cblock;
   a.cwarp = h->d_citems;
   a.n_cwarp = h->n_cwarp;
+  a.warp_claim = h->tune.warp_claim;
   a.pidx = h->d_pidx;
   a.cursor = h->d_cursor;
   a.seg_cycles = (h->opts.record_timings >= 2 || h->collect_cycles) ? h->d_seg_cycles : nullptr;
   a.cw_iterate = h->cw_iterate;
   a.cw_decode = h->cw_decode;
   a.cw_count = h->cw_count;
-  a.ktime = h->collect_cycles ? h->d_ktime : nullptr;
+  a.ktime = (h->collect_cycles || h->measure_busy) ? h->d_ktime : nullptr;
   a.seg_changed = h->learner ? h->d_seg_changed : nullptr;
   a.cms_thr = h->opts.cms_threshold;
   for (int r = 0; r < kCmsDepth; r++) a.seeds[r] = h->seeds[r];
@@ -911,6 +915,147 @@ lpa_status lpa_set_dispatch(lpa_handle *h, int dispatch, int force_variant) {
     apply_dispatch(h, dispatch == LPA_DISPATCH_FORCE ? LPA_DISPATCH_FORCE : LPA_DISPATCH_FIXED, force_variant);
     check(h, cudaStreamSynchronize(h->stream), "dispatch");
   } catch (const Fail &f) {
+    return guard(h, f);
+  }
+  return LPA_OK;
+}
+
+static bool tune_valid(const lpa_tune &t) {
+  return t.group_positions >= 1 && t.group_positions <= 32 && t.warp_positions >= 1 && t.warp_positions <= 32 &&
+         t.warp_max_degree >= 32 && t.warp_max_degree <= kCountWarpMax && t.warp_claim >= 1 && t.warp_claim <= 8;
+}
+
+// One iteration from the current labels, repeated; the labels are left as
+// they were (an iteration reads one buffer and writes the other, and the
+// buffer pointer is put back).  Returns the least kernel busy time (ms) on
+// the GPU clock, or a negative value when an iteration failed.
+static double tune_trial(lpa_handle *h, int repeats) {
+  const int cur = h->cur;
+  double best = -1;
+  h->measure_busy = true;
+  for (int r = 0; r < repeats; r++) {
+    check(h, cudaMemsetAsync(h->d_ktime, 0xFF, 3 * sizeof(unsigned long long), h->stream), "clear spans");
+    check(h, cudaMemsetAsync(h->d_ktime + 3, 0, 3 * sizeof(unsigned long long), h->stream), "clear spans");
+    check(h, cudaMemsetAsync(h->d_changed, 0, sizeof(unsigned long long), h->stream), "clear counter");
+    check(h, cudaMemsetAsync(h->d_work, 0, 4 * sizeof(uint32_t), h->stream), "clear work counters");
+    enqueue_iteration(h, h->d_changed, h->d_work);
+    h->cur = cur;
+    check(h, cudaGetLastError(), "tuning iteration");
+    if (take_device_error(h) != LPA_OK) {
+      h->measure_busy = false;
+      return -1;
+    }
+    unsigned long long span[6];
+    check(h, cudaMemcpy(span, h->d_ktime, sizeof(span), cudaMemcpyDeviceToHost), "read spans");
+    double busy = 0;
+    for (int k = 0; k < 3; k++)
+      if (span[3 + k] > span[k]) busy += double(span[3 + k] - span[k]) * 1e-6;
+    if (best < 0 || busy < best) best = busy;
+  }
+  h->measure_busy = false;
+  return best;
+}
+
+// The cache key: GPU, graph, sketch threshold and plan.
+static std::string tune_key(const lpa_handle *h) {
+  cudaDeviceProp pr{};
+  if (cudaGetDeviceProperties(&pr, h->device) != cudaSuccess) cudaGetLastError();
+  std::string gpu = pr.name;
+  for (char &ch : gpu)
+    if (ch == ' ' || ch == '|') ch = '_';
+  uint64_t fnv = 1469598103934665603ull;
+  for (uint8_t v : h->variant) fnv = (fnv ^ v) * 1099511628211ull;
+  uint64_t arcs = 0;
+  for (const auto &sg : h->segs) arcs += sg.arcs;
+  char buf[512];
+  std::snprintf(buf, sizeof(buf), "%s|sm%d|n%llu|nc%llu|arcs%llu|cms%u|plan%016llx", gpu.c_str(), pr.multiProcessorCount,
+                (unsigned long long)h->n, (unsigned long long)h->n_c, (unsigned long long)arcs,
+                h->opts.cms_threshold, (unsigned long long)fnv);
+  return buf;
+}
+
+lpa_status lpa_get_tune(lpa_handle *h, lpa_tune *out) {
+  if (!h || !out) return LPA_ERR_INVALID_ARG;
+  *out = h->tune;
+  return LPA_OK;
+}
+
+lpa_status lpa_set_tune(lpa_handle *h, const lpa_tune *t) {
+  if (!h || !t || !tune_valid(*t)) return LPA_ERR_INVALID_ARG;
+  try {
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    h->tune = *t;
+    lpa_rt_apply_variants(h);
+  } catch (const Fail &f) {
+    return guard(h, f);
+  }
+  return LPA_OK;
+}
+
+lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_tune *out) {
+  if (!h) return LPA_ERR_INVALID_ARG;
+  if (repeats <= 0) repeats = 2;
+  try {
+    check(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const std::string key = tune_key(h);
+    bool found = false;
+    if (cache_path) {
+      std::ifstream in(cache_path);
+      std::string line;
+      while (std::getline(in, line)) {
+        std::istringstream ls(line);
+        std::string k;
+        lpa_tune t{};
+        if (ls >> k >> t.group_positions >> t.warp_positions >> t.warp_max_degree >> t.warp_claim && k == key &&
+            tune_valid(t)) {
+          h->tune = t;
+          found = true;
+        }
+      }
+    }
+    if (found) {
+      lpa_rt_apply_variants(h);
+    } else if (h->n_cblock + h->n_cwarp > 0) {
+      // coordinate descent, two sweeps; a candidate must win by 0.5 %
+      lpa_tune best = h->tune;
+      double best_ms = tune_trial(h, repeats);
+      if (best_ms < 0) throw Fail{LPA_ERR_CUDA, "autotune: " + h->last_error};
+      static const uint32_t groups[] = {8, 16, 24, 32}, warps[] = {1, 2, 4, 8, 16},
+                            degs[] = {63, 127, 255, kCountWarpMax}, claims[] = {1, 2, 4, 8};
+      for (int sweep = 0; sweep < 2; sweep++) {
+        for (int knob = 0; knob < 4; knob++) {
+          const uint32_t *vals = knob == 0 ? groups : knob == 1 ? warps : knob == 2 ? degs : claims;
+          const int nv = knob == 1 ? 5 : 4;
+          for (int i = 0; i < nv; i++) {
+            lpa_tune cand = best;
+            uint32_t &slot = knob == 0 ? cand.group_positions
+                             : knob == 1 ? cand.warp_positions
+                             : knob == 2 ? cand.warp_max_degree
+                                         : cand.warp_claim;
+            if (slot == vals[i]) continue;
+            slot = vals[i];
+            h->tune = cand;
+            lpa_rt_apply_variants(h);
+            const double ms = tune_trial(h, repeats);
+            if (ms < 0) throw Fail{LPA_ERR_CUDA, "autotune: " + h->last_error};
+            if (ms < best_ms * 0.995) {
+              best = cand;
+              best_ms = ms;
+            }
+          }
+        }
+      }
+      h->tune = best;
+      lpa_rt_apply_variants(h);
+      if (cache_path) {
+        std::ofstream o(cache_path, std::ios::app);
+        o << key << ' ' << best.group_positions << ' ' << best.warp_positions << ' ' << best.warp_max_degree << ' '
+          << best.warp_claim << ' ' << best_ms << '\n';
+      }
+    }
+    if (out) *out = h->tune;
+  } catch (const Fail &f) {
+    h->measure_busy = false;
     return guard(h, f);
   }
   return LPA_OK;
