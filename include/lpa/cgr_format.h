@@ -68,6 +68,14 @@ struct CgrGraph {
 void cgr_encode(const CsrView &g, const CgrParams &p, int small_thresh, int large_thresh,
                 CgrGraph &out, int threads = 0);
 
+// The same encoding on a GPU (byte-identical output): the per-vertex bit
+// sizing and writing run one thread per compressed vertex on `device`; the
+// position order, offsets prefix sum and small CSR stay on the host.  Only
+// the reference parameters (3, 4, 256, 256).  Throws std::invalid_argument on
+// unsupported input and std::runtime_error on a CUDA failure.
+void cgr_encode_gpu(const CsrView &g, const CgrParams &p, int small_thresh, int large_thresh, CgrGraph &out,
+                    int device = 0);
+
 // Bits one vertex occupies (same parameters); used by tests and planners.
 uint64_t cgr_vertex_bits(const uint32_t *nbrs, uint64_t deg, uint32_t node, const CgrParams &p);
 

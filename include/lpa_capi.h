@@ -251,6 +251,10 @@ lpa_status lpa_hg_read_edge_list(const char *path, int one_way, lpa_host_graph *
 lpa_status lpa_hg_write_edge_list(lpa_host_graph *g, const char *path, int both_arcs);
 /* CgrCompressor(3, 4, 256, 256) + write_cgr(path, small_thresh, large_thresh). */
 lpa_status lpa_hg_compress(lpa_host_graph *g, int small_thresh, int large_thresh, int threads);
+/* The same compression on a GPU, byte-identical to lpa_hg_compress: bit
+ * sizing and writing run one thread per compressed vertex on `device`.  Only
+ * the reference parameters.  LPA_ERR_CUDA when the device fails or is absent. */
+lpa_status lpa_hg_compress_gpu(lpa_host_graph *g, int small_thresh, int large_thresh, int device);
 /* Loads the reference's compressed files (64-bit offsets). */
 lpa_status lpa_hg_load_cgr(const char *base, int small_thresh, lpa_host_graph **out);
 lpa_status lpa_hg_write_cgr(lpa_host_graph *g, const char *base);

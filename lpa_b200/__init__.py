@@ -184,6 +184,7 @@ def lib():
     _sig(L, "lpa_hg_read_edge_list", [C.c_char_p, C.c_int, PP])
     _sig(L, "lpa_hg_write_edge_list", [P, C.c_char_p, C.c_int])
     _sig(L, "lpa_hg_compress", [P, C.c_int, C.c_int, C.c_int])
+    _sig(L, "lpa_hg_compress_gpu", [P, C.c_int, C.c_int, C.c_int])
     _sig(L, "lpa_hg_load_cgr", [C.c_char_p, C.c_int, PP])
     _sig(L, "lpa_hg_write_cgr", [P, C.c_char_p])
     _sig(L, "lpa_hg_write_csr", [P, C.c_char_p])
@@ -277,8 +278,12 @@ class HostGraph:
     def write_edge_list(self, path, both_arcs: bool):
         _check(lib().lpa_hg_write_edge_list(self._h, str(path).encode(), int(both_arcs)), "write_edge_list")
 
-    def compress(self, small_thresh=0, large_thresh=128, threads=0):
-        _check(lib().lpa_hg_compress(self._h, small_thresh, large_thresh, threads), "compress")
+    def compress(self, small_thresh=0, large_thresh=128, threads=0, device=None):
+        """CGR-compress the CSR on the host (threads) or, with device, on that GPU."""
+        if device is None:
+            _check(lib().lpa_hg_compress(self._h, small_thresh, large_thresh, threads), "compress")
+        else:
+            _check(lib().lpa_hg_compress_gpu(self._h, small_thresh, large_thresh, int(device)), "compress_gpu")
         return self
 
     def write_cgr(self, base):

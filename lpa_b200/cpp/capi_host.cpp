@@ -157,6 +157,24 @@ lpa_status lpa_hg_compress(lpa_host_graph *g, int small_thresh, int large_thresh
   });
 }
 
+lpa_status lpa_hg_compress_gpu(lpa_host_graph *g, int small_thresh, int large_thresh, int device) {
+  if (!g || !g->has_csr) return LPA_ERR_INVALID_ARG;
+  try {
+    lpa::CgrParams p;  // (3, 4, 256, 256), src/file.cpp:84
+    lpa::CgrGraph out;
+    lpa::cgr_encode_gpu(g->csr.view(), p, small_thresh, large_thresh, out, device);
+    g->cgr = std::move(out);
+    g->has_cgr = true;
+    return LPA_OK;
+  } catch (const std::bad_alloc &) {
+    return LPA_ERR_OOM;
+  } catch (const std::invalid_argument &) {
+    return LPA_ERR_INVALID_ARG;
+  } catch (const std::exception &) {
+    return LPA_ERR_CUDA;  // the device failed (or there is none)
+  }
+}
+
 lpa_status lpa_hg_load_cgr(const char *base, int small_thresh, lpa_host_graph **out) {
   if (!out || !base) return LPA_ERR_INVALID_ARG;
   return guarded([&]() {
