@@ -382,7 +382,7 @@ def main():
     def timed_region(steps):
         """K iterations; device time of each from the library's CUDA events."""
         dev = 0.0
-        kern = np.zeros(3)
+        kern = np.zeros(4)
         for _ in range(steps):
             if flush:
                 with torch.cuda.stream(stream):
@@ -390,7 +390,7 @@ def main():
             p.iterate()
             s = p.stats()
             dev += s.last_iter_ms
-            kern += np.array([s.decode_ms, s.count_ms, s.iterate_ms])
+            kern += np.array([s.decode_ms, s.count_ms, s.packed_ms, s.iterate_ms])
         return dev, kern
 
     # fixed degree-bucket plan (the reference's buckets): warm-up, then the
@@ -477,13 +477,14 @@ def main():
                        "timed_iterations": f"1..{args.steps} from the initial labels",
                        "l2": "L2 flushed between iterations" if flush else "inputs larger than L2",
                        "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "kernel": "iteration (k_decode_two_pass + k_count_two_pass + k_iterate)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "iteration (k_decode_two_pass + k_count_two_pass + k_packed + k_iterate)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "bytes_per_launch": b_alg, "ms_per_launch": ms_per_step,
                          "traffic": traffic_summary(args.workload),
                          "kernel_ms": {"k_decode_two_pass": float(kern_avg[0]), "k_count_two_pass": float(kern_avg[1]),
-                                       "k_iterate": float(kern_avg[2])}},
+                                       "k_packed": float(kern_avg[2]), "k_iterate": float(kern_avg[3])}},
             "dispatch": {"mode": args.dispatch,
                          "fixed_value": arcs * args.steps * world / (fixed_ms / 1e3),
                          "fixed_ms_per_step": fixed_ms / args.steps,

@@ -110,6 +110,7 @@ typedef struct lpa_stats {
   double decode_ms;                 /* two-pass decode kernel, last iteration */
   double iterate_ms;                /* persistent iteration kernel, last iteration */
   double count_ms;                  /* two-pass count kernel, last iteration */
+  double packed_ms;                 /* lane-per-vertex kernel of the tiny bucket, last iteration */
 } lpa_stats;
 
 /* ---------------------------------------------------------------- basics -- */

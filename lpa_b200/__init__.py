@@ -134,6 +134,7 @@ class Stats(C.Structure):
         ("decode_ms", C.c_double),
         ("iterate_ms", C.c_double),
         ("count_ms", C.c_double),
+        ("packed_ms", C.c_double),
     ]
 
 

@@ -363,8 +363,9 @@ void lpa_learner_before_iteration(lpa_handle *h) {
   set_plan(h, plan);
   h->collect_cycles = true;
   cudaMemsetAsync(h->d_seg_cycles, 0, std::max<size_t>(1, h->segs.size()) * sizeof(long long), h->stream);
-  cudaMemsetAsync(h->d_ktime, 0xFF, 3 * sizeof(unsigned long long), h->stream);  // starts: none yet
-  cudaMemsetAsync(h->d_ktime + 3, 0, 3 * sizeof(unsigned long long), h->stream);  // ends
+  cudaMemsetAsync(h->d_ktime, 0xFF, lpa_dev::kBusyKernels * sizeof(unsigned long long), h->stream);  // starts
+  cudaMemsetAsync(h->d_ktime + lpa_dev::kBusyKernels, 0, lpa_dev::kBusyKernels * sizeof(unsigned long long),
+                  h->stream);  // ends
   std::swap(h->d_seg_changed, h->d_seg_changed_prev);
   cudaMemsetAsync(h->d_seg_changed, 0, std::max<size_t>(1, h->segs.size()) * sizeof(uint32_t), h->stream);
 }
@@ -378,11 +379,11 @@ void lpa_learner_after_iteration(lpa_handle *h) {
   // iteration, it leaves out host-side gaps between launches, which a tool
   // such as a profiler can stretch by orders of magnitude.
   double t = h->last_iter_ms;
-  unsigned long long span[6];
+  unsigned long long span[2 * lpa_dev::kBusyKernels];
   if (cudaMemcpy(span, h->d_ktime, sizeof(span), cudaMemcpyDeviceToHost) == cudaSuccess) {
     double busy = 0;
-    for (int k = 0; k < 3; k++)
-      if (span[3 + k] > span[k]) busy += double(span[3 + k] - span[k]) * 1e-6;
+    for (int k = 0; k < lpa_dev::kBusyKernels; k++)
+      if (span[lpa_dev::kBusyKernels + k] > span[k]) busy += double(span[lpa_dev::kBusyKernels + k] - span[k]) * 1e-6;
     if (busy > 0) t = busy;
   } else {
     cudaGetLastError();

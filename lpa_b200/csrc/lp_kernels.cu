@@ -754,7 +754,7 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, un
 __device__ __forceinline__ void busy_mark(const IterArgs &a, int kernel, bool end) {
   if (a.ktime && (threadIdx.x & 31u) == 0) {
     const unsigned long long t = global_ns();
-    if (end) atomicMax(a.ktime + 3 + kernel, t);
+    if (end) atomicMax(a.ktime + kBusyKernels + kernel, t);
     else atomicMin(a.ktime + kernel, t);
   }
 }
@@ -902,6 +902,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchArgs b) {
       ia.pidx = nullptr;
       ia.cursor = nullptr;
       ia.ktime = nullptr;
+      ia.packed = nullptr;
+      ia.n_packed = 0;
       ia.gtab = b.gtab;
       ia.gtab_slots = b.gtab_slots;
     }
@@ -963,6 +965,68 @@ __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs) {
       bg.labs1[v] = uint32_t(v);
     }
   }
+}
+
+// V2 (several vertices per warp) at its limit for the tiny bucket: one lane
+// per position, 32 vertices per warp.  The lane walks its vertex's whole bit
+// range (or its small-CSR list), gathering each label as soon as its id is
+// decoded, then takes the most frequent of its <= 15 labels (smallest on
+// ties) by pairwise counts.  No shared memory, no warp-wide steps.
+__global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
+  const DevGraph &g = a.g;
+  const Ctx c = resolve(a);
+  busy_mark(a, 3, false);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long changed = 0;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n_packed; i += nw) {
+    const long long t0 = clock64();
+    const PackedChunk ch = a.packed[i];
+    const uint32_t p = ch.p0 + lane;
+    uint32_t mine = 0;
+    if (lane < ch.np) {
+      const uint32_t node = g.vertices[p];
+      const uint32_t d = g.deg[p];
+      const uint32_t old = ld_label(c, node);
+      uint32_t lab[kPackedMaxDeg];
+      uint32_t k = 0;
+      bool bad = d > kPackedMaxDeg;
+      if (!bad && p < g.n_c) {
+        const int64_t r = walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], node, g.n, [&](uint32_t id) {
+          if (k < kPackedMaxDeg) lab[k] = ld_label(c, id);
+          k++;
+        });
+        bad = r != int64_t(d);
+      } else if (!bad) {
+        const uint32_t *ids = g.small_nbr + g.small_off[p - g.n_c];
+        for (; k < d; k++) lab[k] = ld_label(c, ids[k]);
+      }
+      if (bad) {
+        set_error(a.err, kErrBadStream);
+      } else if (d) {
+        uint64_t best = 0;
+        for (uint32_t x = 0; x < d; x++) {
+          uint32_t cnt = 0;
+          for (uint32_t y = 0; y < d; y++) cnt += lab[y] == lab[x];
+          const uint64_t cand = pack_best(cnt, lab[x]);
+          best = cand > best ? cand : best;
+        }
+        const uint32_t nl = best_label(best);
+        c.lab_out[node] = nl;
+        mine = nl != old;
+      }
+    }
+    changed += mine;
+    const uint32_t sc = __reduce_add_sync(kFull, mine);
+    if (lane == 0) {
+      if (a.seg_changed && sc) atomicAdd(a.seg_changed + ch.seg, sc);
+      if (a.seg_cycles)
+        atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + ch.seg),
+                  (unsigned long long)((clock64() - t0) * a.cw_packed));
+    }
+  }
+  busy_mark(a, 3, true);
+  flush_changed(c.changed, changed);
 }
 
 // Two-pass variant, pass 1.  Every 256-bit segment of the two-pass positions

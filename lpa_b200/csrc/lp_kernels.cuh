@@ -74,6 +74,15 @@ constexpr uint32_t kCountBlockSlots = kWarps * kCountWarpSlots;  // the warps' t
 constexpr uint32_t kCountBlockMax = 2047;
 constexpr uint32_t kCountSmemBytes = kCountBlockSlots * 8;        // 32 KB
 
+// Work of k_packed: up to 32 consecutive positions of one plan segment whose
+// degrees are all <= kPackedMaxDeg, one lane each.
+struct PackedChunk {
+  uint32_t p0, np, seg, pad;
+};
+constexpr uint32_t kPackedMaxDeg = 15;  // the tiny bucket (degree < 16)
+
+constexpr int kBusyKernels = 4;  // kernels of an iteration with a busy span (IterArgs::ktime)
+
 struct IterArgs {
   DevGraph g;
   uint32_t *labs0, *labs1;      // the two label buffers
@@ -96,6 +105,9 @@ struct IterArgs {
   const CountItem *cwarp;
   uint32_t n_cwarp;
   uint32_t warp_claim;          // warp items a warp of the count pass claims at once
+  const PackedChunk *packed;    // k_packed work
+  uint32_t n_packed;
+  uint32_t cw_packed;           // cost weight of a k_packed warp-cycle (as cw_iterate)
   uint32_t *cursor;             // per compressed position: labels written by the pre-pass (pass 2 resets)
   long long *seg_cycles;        // per-segment device cycles (nullptr: off)
   // weights of one warp-cycle of k_iterate / k_decode_two_pass /
@@ -103,8 +115,9 @@ struct IterArgs {
   // SM), so a booked unit is the same share of an SM whichever kernel spent it
   uint32_t cw_iterate, cw_decode, cw_count;
   // nullptr, or the busy span of each kernel of the iteration on the GPU's
-  // clock (ns): ktime[k] = earliest warp start, ktime[3 + k] = latest warp end,
-  // k = 0 k_decode_two_pass, 1 k_count_two_pass, 2 k_iterate
+  // clock (ns): ktime[k] = earliest warp start, ktime[kBusyKernels + k] =
+  // latest warp end, k = 0 k_decode_two_pass, 1 k_count_two_pass, 2 k_iterate,
+  // 3 k_packed
   unsigned long long *ktime;
   uint32_t *seg_changed;        // per-segment changed counts (nullptr: off)
   uint32_t cms_thr;             // 0: no sketch
@@ -159,6 +172,8 @@ __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs);
 
 __global__ void k_iterate(IterArgs a);
 __global__ void k_decode_two_pass(IterArgs a);
+// V2 for tiny vertices: a lane per vertex.
+__global__ void k_packed(IterArgs a);
 // Two-pass variant, pass 2: counts the labels the pre-pass wrote.
 __global__ void k_count_two_pass(IterArgs a);
 

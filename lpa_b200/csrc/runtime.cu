@@ -215,6 +215,7 @@ static void upload_lists(lpa_handle *h) {
   std::vector<WorkItem> heavy, light;
   std::vector<DecodeGroup> groups;
   std::vector<BlockItem> cblock;
+  std::vector<PackedChunk> packed;
   std::vector<CountItem> cwarp;
   const uint32_t cms = h->opts.cms_threshold;
   const uint32_t wmax = h->tune.warp_max_degree;  // above: a block item
@@ -261,6 +262,9 @@ static void upload_lists(lpa_handle *h) {
       }
     } else if (block) {
       heavy.push_back(make_item(h, uint32_t(s), si.begin, si.end, tp));
+    } else if (v == LPA_VARIANT_PACKED && si.max_deg <= kPackedMaxDeg) {
+      for (uint32_t p0 = si.begin; p0 < si.end; p0 += 32)
+        packed.push_back(PackedChunk{p0, std::min(si.end - p0, 32u), uint32_t(s), 0});
     } else {
       const uint32_t chunks = (si.end - si.begin + 31) / 32;
       for (uint32_t c = 0; c < chunks; c++) {
@@ -339,6 +343,9 @@ static void upload_lists(lpa_handle *h) {
   regrow(h->d_groups, h->groups_cap, groups.size(), "decode groups");
   regrow(h->d_citems, h->citems_cap, citems.size(), "count items");
   regrow(h->d_cblock, h->cblock_cap, cblock.size(), "count block items");
+  regrow(h->d_packed, h->packed_cap, packed.size(), "packed chunks");
+  h2d(h, h->d_packed, packed.data(), packed.size(), "upload packed chunks");
+  h->n_packed = uint32_t(packed.size());
   h2d(h, h->d_cblock, cblock.data(), cblock.size(), "upload count block items");
   h2d(h, h->d_citems, citems.data(), citems.size(), "upload count items");
   h2d(h, h->d_items, all.data(), all.size(), "upload work items");
@@ -438,7 +445,7 @@ static void build_plan(lpa_handle *h) {
   h2d(h, h->d_segs, ds.data(), ds.size(), "upload segments");
   check(h, cudaStreamSynchronize(h->stream), "upload segments");
   h->d_seg_cycles = dalloc<long long>(h, h->segs.size(), "segment cycles");
-  h->d_ktime = dalloc<unsigned long long>(h, 6, "kernel busy spans");
+  h->d_ktime = dalloc<unsigned long long>(h, 2 * kBusyKernels, "kernel busy spans");
   check(h, cudaMemsetAsync(h->d_seg_cycles, 0, std::max<size_t>(1, h->segs.size()) * sizeof(long long), h->stream),
         "clear cycles");
 
@@ -485,6 +492,9 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.cwarp = h->d_citems;
   a.n_cwarp = h->n_cwarp;
   a.warp_claim = h->tune.warp_claim;
+  a.packed = h->d_packed;
+  a.n_packed = h->n_packed;
+  a.cw_packed = h->cw_packed;
   a.pidx = h->d_pidx;
   a.cursor = h->d_cursor;
   a.seg_cycles = (h->opts.record_timings >= 2 || h->collect_cycles) ? h->d_seg_cycles : nullptr;
@@ -509,22 +519,36 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
 static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32_t *work) {
   const bool timed = h->opts.record_timings && h->events_ready;
   const IterArgs a = iter_args(h, changed, work);
-  if (timed) cudaEventRecord(h->ev[0], h->stream);
+  // events only around the kernels that run: an event costs a few us of
+  // device time, which small graphs would otherwise count
+  int ne = 0;
+  auto mark = [&](int kernel) {
+    if (!timed) return;
+    h->ev_kernel[ne] = kernel;
+    cudaEventRecord(h->ev[ne++], h->stream);
+  };
+  mark(-1);
   if (h->n_groups) {
     k_decode_two_pass<<<h->grid_decode, kThreads, 0, h->stream>>>(a);
     h->launches++;
+    mark(0);
   }
-  if (timed) cudaEventRecord(h->ev[1], h->stream);
   if (h->n_cblock + h->n_cwarp) {
     k_count_two_pass<<<h->grid_count, kThreads, kCountSmemBytes, h->stream>>>(a);
     h->launches++;
+    mark(1);
   }
-  if (timed) cudaEventRecord(h->ev[2], h->stream);
+  if (h->n_packed) {
+    k_packed<<<h->grid_packed, kThreads, 0, h->stream>>>(a);
+    h->launches++;
+    mark(2);
+  }
   if (h->n_heavy + h->n_light) {
     k_iterate<<<h->grid, kThreads, kSmemBytes, h->stream>>>(a);
     h->launches++;
+    mark(3);
   }
-  if (timed) cudaEventRecord(h->ev[3], h->stream);
+  h->ev_used = ne;
   h->cur ^= 1;
 }
 
@@ -539,10 +563,13 @@ static void collect_times(lpa_handle *h) {
     return double(t);
   };
   for (int v = 0; v < 4; v++) h->variant_ms[v] = 0;
-  h->decode_ms = ms(0, 1);
-  h->count_ms = ms(1, 2);
-  h->iterate_ms = ms(2, 3);
-  h->last_iter_ms = ms(0, 3);
+  double k_ms[4] = {0, 0, 0, 0};  // pre-pass, count pass, k_packed, k_iterate
+  for (int e = 1; e < h->ev_used; e++) k_ms[h->ev_kernel[e]] = ms(e - 1, e);
+  h->decode_ms = k_ms[0];
+  h->count_ms = k_ms[1];
+  h->packed_ms = k_ms[2];
+  h->iterate_ms = k_ms[3];
+  h->last_iter_ms = h->ev_used > 1 ? ms(0, h->ev_used - 1) : 0.0;
 }
 
 // ------------------------------------------------------------------ C ABI --
@@ -637,6 +664,10 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     h->cw_iterate = weight(h->occ);
     h->cw_count = weight(occ_count);
     h->cw_decode = weight(occ_decode);
+    int occ_packed = 1;
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_packed, k_packed, kThreads, 0), "occupancy");
+    h->grid_packed = h->num_sms * std::max(1, occ_packed);
+    h->cw_packed = weight(occ_packed);
 
     h->n = n;
     h->n_c = n_c;
@@ -846,6 +877,7 @@ lpa_status lpa_get_stats(lpa_handle *h, lpa_stats *st) {
   st->decode_ms = h->decode_ms;
   st->iterate_ms = h->iterate_ms;
   st->count_ms = h->count_ms;
+  st->packed_ms = h->packed_ms;
   for (int v = 0; v < 4; v++) st->variant_ms[v] = h->variant_ms[v];
   for (size_t s = 0; s < h->segs.size(); s++) {
     st->variant_segments[h->variant[s]]++;
@@ -934,8 +966,9 @@ static double tune_trial(lpa_handle *h, int repeats) {
   double best = -1;
   h->measure_busy = true;
   for (int r = 0; r < repeats; r++) {
-    check(h, cudaMemsetAsync(h->d_ktime, 0xFF, 3 * sizeof(unsigned long long), h->stream), "clear spans");
-    check(h, cudaMemsetAsync(h->d_ktime + 3, 0, 3 * sizeof(unsigned long long), h->stream), "clear spans");
+    check(h, cudaMemsetAsync(h->d_ktime, 0xFF, kBusyKernels * sizeof(unsigned long long), h->stream), "clear spans");
+    check(h, cudaMemsetAsync(h->d_ktime + kBusyKernels, 0, kBusyKernels * sizeof(unsigned long long), h->stream),
+          "clear spans");
     check(h, cudaMemsetAsync(h->d_changed, 0, sizeof(unsigned long long), h->stream), "clear counter");
     check(h, cudaMemsetAsync(h->d_work, 0, 4 * sizeof(uint32_t), h->stream), "clear work counters");
     enqueue_iteration(h, h->d_changed, h->d_work);
@@ -945,11 +978,11 @@ static double tune_trial(lpa_handle *h, int repeats) {
       h->measure_busy = false;
       return -1;
     }
-    unsigned long long span[6];
+    unsigned long long span[2 * kBusyKernels];
     check(h, cudaMemcpy(span, h->d_ktime, sizeof(span), cudaMemcpyDeviceToHost), "read spans");
     double busy = 0;
-    for (int k = 0; k < 3; k++)
-      if (span[3 + k] > span[k]) busy += double(span[3 + k] - span[k]) * 1e-6;
+    for (int k = 0; k < kBusyKernels; k++)
+      if (span[kBusyKernels + k] > span[k]) busy += double(span[kBusyKernels + k] - span[k]) * 1e-6;
     if (best < 0 || busy < best) best = busy;
   }
   h->measure_busy = false;

@@ -85,6 +85,11 @@ struct lpa_handle {
   uint32_t *d_cursor = nullptr;              // per compressed position: pre-pass output cursor
   lpa_dev::CountItem *d_citems = nullptr;    // count-pass warp items
   lpa_dev::BlockItem *d_cblock = nullptr;    // count-pass block items
+  lpa_dev::PackedChunk *d_packed = nullptr;  // k_packed work
+  uint32_t n_packed = 0;
+  size_t packed_cap = 0;
+  int grid_packed = 0;
+  uint32_t cw_packed = 1;
   size_t cblock_cap = 0;
   std::vector<uint32_t> h_vertices;          // vertex id of every compressed position
   uint32_t n_cblock = 0, n_cwarp = 0;
@@ -117,9 +122,11 @@ struct lpa_handle {
   std::vector<uint64_t> history;
   double last_iter_ms = 0;
   double variant_ms[4] = {0, 0, 0, 0};
-  double decode_ms = 0, iterate_ms = 0, count_ms = 0;
+  double decode_ms = 0, iterate_ms = 0, count_ms = 0, packed_ms = 0;
   bool collect_cycles = false;  // per-segment cycles for the cost model
-  cudaEvent_t ev[4] = {};  // iteration start, after the pre-pass, after the count pass, iteration end
+  cudaEvent_t ev[5] = {};  // iteration start, then one after each kernel that ran
+  int ev_kernel[5] = {};   // which kernel each event follows (0 pre-pass, 1 count, 2 k_packed, 3 k_iterate)
+  int ev_used = 0;
   bool events_ready = false;
   uint64_t device_bytes = 0;
   std::vector<void *> allocations;
