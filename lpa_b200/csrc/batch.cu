@@ -180,6 +180,8 @@ lpa_status lpa_batch_create(const lpa_graph_desc *graphs, size_t num_graphs, con
         if (b->opts.dispatch == LPA_DISPATCH_FORCE && b->opts.force_variant != LPA_VARIANT_TWO_PASS &&
             lpa_rt::variant_capable(b->opts.force_variant, sg, b->opts.cms_threshold))
           v = b->opts.force_variant;
+        // tiny packed segments run one thread per position
+        if (v == LPA_VARIANT_PACKED && sg.max_deg <= kPackedMaxDeg) v = kVarPackedLanes;
         all_var.push_back(uint8_t(v));
       }
       for (uint64_t p = 0; p < b->n[gi]; p++) {

@@ -833,6 +833,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
   flush_changed(c.changed, changed);
 }
 
+__device__ __forceinline__ uint32_t packed_vertex(const IterArgs &a, const Ctx &c, uint32_t p);
+
 // Many graphs, one persistent launch.  A ring queue holds (graph,
 // iteration, segment) items; iteration 0 of every graph is queued by the
 // host.  The block that finishes the last item of a graph's iteration reads
@@ -919,6 +921,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchArgs b) {
     const int v = ia.seg_var[s];
     if (v == kVarBlock || v == kVarTwoPass) {
       for (uint32_t p = sg.begin; p < sg.end; p++) heavy_vertex(ia, c, sh, stage, tab, s, p, false, changed);
+    } else if (v == kVarPackedLanes) {
+      // a tiny segment: one thread per position (<= 256 positions)
+      if (sg.begin + t < sg.end) changed += packed_vertex(ia, c, sg.begin + t);
     } else {
       const uint32_t p0 = sg.begin + warp * 32u;  // light segments hold at most 8 chunks
       if (p0 < sg.end) light_chunk(ia, c, wstage, wslots, wepoch, s, p0, min(sg.end, p0 + 32u), v, changed);
@@ -967,13 +972,49 @@ __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs) {
   }
 }
 
-// V2 (several vertices per warp) at its limit for the tiny bucket: one lane
-// per position, 32 vertices per warp.  The lane walks its vertex's whole bit
-// range (or its small-CSR list), gathering each label as soon as its id is
-// decoded, then takes the most frequent of its <= 15 labels (smallest on
-// ties) by pairwise counts.  No shared memory, no warp-wide steps.
-__global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
+// One vertex of degree <= kPackedMaxDeg by one thread: it walks the vertex's
+// whole bit range (or its small-CSR list), gathering each label as soon as
+// its id is decoded, then takes the most frequent of its labels (smallest on
+// ties) by pairwise counts.  Returns 1 when the label changed.
+__device__ __forceinline__ uint32_t packed_vertex(const IterArgs &a, const Ctx &c, uint32_t p) {
   const DevGraph &g = a.g;
+  const uint32_t node = g.vertices[p];
+  const uint32_t d = g.deg[p];
+  const uint32_t old = ld_label(c, node);
+  uint32_t lab[kPackedMaxDeg];
+  uint32_t k = 0;
+  bool bad = d > kPackedMaxDeg;
+  if (!bad && p < g.n_c) {
+    const int64_t r = walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], node, g.n, [&](uint32_t id) {
+      if (k < kPackedMaxDeg) lab[k] = ld_label(c, id);
+      k++;
+    });
+    bad = r != int64_t(d);
+  } else if (!bad) {
+    const uint32_t *ids = g.small_nbr + g.small_off[p - g.n_c];
+    for (; k < d; k++) lab[k] = ld_label(c, ids[k]);
+  }
+  if (bad) {
+    set_error(a.err, kErrBadStream);
+    return 0;
+  }
+  if (d == 0) return 0;
+  uint64_t best = 0;
+  for (uint32_t x = 0; x < d; x++) {
+    uint32_t cnt = 0;
+    for (uint32_t y = 0; y < d; y++) cnt += lab[y] == lab[x];
+    const uint64_t cand = pack_best(cnt, lab[x]);
+    best = cand > best ? cand : best;
+  }
+  const uint32_t nl = best_label(best);
+  c.lab_out[node] = nl;
+  return nl != old;
+}
+
+// V2 (several vertices per warp) at its limit for the tiny bucket: one lane
+// per position (packed_vertex), 32 vertices per warp.  No shared memory, no
+// warp-wide steps.
+__global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
   const Ctx c = resolve(a);
   busy_mark(a, 3, false);
   const uint32_t lane = threadIdx.x & 31u;
@@ -982,40 +1023,7 @@ __global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
   for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n_packed; i += nw) {
     const long long t0 = clock64();
     const PackedChunk ch = a.packed[i];
-    const uint32_t p = ch.p0 + lane;
-    uint32_t mine = 0;
-    if (lane < ch.np) {
-      const uint32_t node = g.vertices[p];
-      const uint32_t d = g.deg[p];
-      const uint32_t old = ld_label(c, node);
-      uint32_t lab[kPackedMaxDeg];
-      uint32_t k = 0;
-      bool bad = d > kPackedMaxDeg;
-      if (!bad && p < g.n_c) {
-        const int64_t r = walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], node, g.n, [&](uint32_t id) {
-          if (k < kPackedMaxDeg) lab[k] = ld_label(c, id);
-          k++;
-        });
-        bad = r != int64_t(d);
-      } else if (!bad) {
-        const uint32_t *ids = g.small_nbr + g.small_off[p - g.n_c];
-        for (; k < d; k++) lab[k] = ld_label(c, ids[k]);
-      }
-      if (bad) {
-        set_error(a.err, kErrBadStream);
-      } else if (d) {
-        uint64_t best = 0;
-        for (uint32_t x = 0; x < d; x++) {
-          uint32_t cnt = 0;
-          for (uint32_t y = 0; y < d; y++) cnt += lab[y] == lab[x];
-          const uint64_t cand = pack_best(cnt, lab[x]);
-          best = cand > best ? cand : best;
-        }
-        const uint32_t nl = best_label(best);
-        c.lab_out[node] = nl;
-        mine = nl != old;
-      }
-    }
+    const uint32_t mine = lane < ch.np ? packed_vertex(a, c, ch.p0 + lane) : 0u;
     changed += mine;
     const uint32_t sc = __reduce_add_sync(kFull, mine);
     if (lane == 0) {

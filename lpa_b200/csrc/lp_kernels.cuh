@@ -13,7 +13,8 @@ enum Variant : int {
   kVarPacked = 1,   // V2: lane-per-vertex decode, several vertices per warp counting (deg <= 32)
   kVarBlock = 2,    // V3: block per vertex, segment-parallel decode, block table / sketch
   kVarTwoPass = 3,  // V4: a decode pass writes a CSR scratch; counting reads it
-  kNumVariants = 4
+  kNumVariants = 4,
+  kVarPackedLanes = 5  // batch plans only: V2 on a tiny segment, one thread per position (packed_vertex)
 };
 
 constexpr int kThreads = 256;             // threads per block of the iteration kernel
