@@ -133,7 +133,11 @@ def run_batch(args, w, rank, world, local):
     arrs = [g.arrays() for g in graphs]
     arcs = [int(len(a["small_graph"])) for a in arrs]
     stream = torch.cuda.Stream(device=device)
-    with L.Batch(graphs, device=local, cms_threshold=w["cms"], stream=stream.cuda_stream) as bt:
+    mode = L.BatchMode.LOCKSTEP if args.batch_mode == "lockstep" else L.BatchMode.QUEUE
+    dispatch = L.Dispatch.LEARNED if args.dispatch == "learned" else L.Dispatch.FIXED
+    with L.Batch(graphs, device=local, cms_threshold=w["cms"], stream=stream.cuda_stream, batch_mode=mode,
+                 dispatch=dispatch) as bt:
+        h = bt.handle()  # lockstep: the concatenated graph's handle
         degs = []
         for g in graphs:  # arcs per graph from the host CSR
             row, _ = g.csr()
@@ -142,6 +146,7 @@ def run_batch(args, w, rank, world, local):
             iters = bt.run(w["iters"], early_exit=True)
         barrier(world, device)
         torch.cuda.synchronize()
+        launches0 = h.stats().launches if h is not None else 0
         clocks = ClockSampler(local)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         total_ms = 0.0
@@ -158,6 +163,9 @@ def run_batch(args, w, rank, world, local):
             bytes_done += sum(algorithmic_bytes(a) * int(k) for a, k in zip(arrs, iters))
         wall = time.perf_counter() - wall0
         clk = clocks.stop()
+        # lockstep: the handle's own count (iteration kernels plus the
+        # two tracker launches); queue: the init kernel and k_batch
+        launches = (h.stats().launches - launches0) if h is not None else 2 * args.steps
         total_ms = max_over_ranks(total_ms, world, device)
         value = work * world / (total_ms / 1e3)
         # end to end: a run plus every graph's labels back to pinned host memory
@@ -182,13 +190,15 @@ def run_batch(args, w, rank, world, local):
                 "config": {"workload": args.workload, "graphs": len(graphs), "vertices": int(sum(a["n"] for a in arrs)),
                            "arcs": int(sum(degs)), "iterations_per_graph": [int(k) for k in iters][:8] + ["..."],
                            "l2": "inputs larger than L2" if sum(algorithmic_bytes(a) for a in arrs) > 2 * L2_BYTES
-                           else "resident", "parallelism": f"replicas x{world}"},
-                "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                           else "resident", "parallelism": f"replicas x{world}", "batch_mode": args.batch_mode,
+                           "dispatch": args.dispatch if h is not None else "fixed"},
+                "roofline": {"bound": "hbm", "kernel": "lockstep iteration kernels" if h is not None else "k_batch",
+                             "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": peak_kind, "traffic": None},
                 "cpu_baseline": None,
                 "e2e": {"value": e2e_work * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": int(4 * sum(a["n"] for a in arrs))},
-                "gpu_launches": 2 * args.steps, "clocks": clk, "wall_s_timed": wall}
+                "gpu_launches": int(launches), "clocks": clk, "wall_s_timed": wall}
         print(json.dumps(line), flush=True)
 
 
@@ -337,6 +347,8 @@ def main():
     ap.add_argument("--dispatch", default="learned", choices=["fixed", "learned"],
                     help="learned: the MLP plan (judged against the fixed buckets, also measured)")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--batch-mode", default="lockstep", choices=["lockstep", "queue"],
+                    help="batched workloads: the concatenated graph in lockstep, or the persistent queue")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

@@ -84,7 +84,13 @@ typedef struct lpa_opts {
   void *stream;            /* cudaStream_t to run on; NULL: the handle makes one */
   int record_timings;      /* 1: per-launch events; 2: also per-segment device cycles */
   int verbose;             /* per-iteration log lines on stdout */
+  int batch_mode;          /* lpa_batch_mode, for lpa_batch_create */
 } lpa_opts;
+
+typedef enum lpa_batch_mode {
+  LPA_BATCH_LOCKSTEP = 0, /* the batch concatenated into one graph, run by one handle */
+  LPA_BATCH_QUEUE = 1     /* one persistent launch fed by a device work queue */
+} lpa_batch_mode;
 
 typedef struct lpa_info {
   uint64_t num_vertices, num_compressed, num_arcs, num_small_arcs;
@@ -264,16 +270,37 @@ lpa_status lpa_hg_write_csr(lpa_host_graph *g, const char *base);
 lpa_status lpa_hg_csr(lpa_host_graph *g, uint64_t *n, const uint64_t **row, const uint32_t **clm);
 /* Fills desc with pointers into g (valid while g lives). */
 lpa_status lpa_hg_desc(lpa_host_graph *g, lpa_graph_desc *desc);
+/* The graphs as one: positions [0, n_c) hold every graph's compressed
+ * positions in graph order, then every graph's small positions; graph k's ids
+ * are shifted by the vertex counts of graphs 0..k-1; the bitstreams are
+ * concatenated bit for bit, so every offset is exact.  A vertex decodes to its
+ * own graph's arcs, shifted, because CGR codes ids relative to the vertex
+ * itself and to each other.  LPA_ERR_CAPACITY when the ids or small arcs
+ * leave 32 bits.  No counterpart in the reference. */
+lpa_status lpa_hg_concat(const lpa_graph_desc *graphs, size_t num_graphs, lpa_host_graph **out);
 lpa_status lpa_hg_free(lpa_host_graph *g);
 
 /* ------------------------------------------------- batched graphs ---------- */
-/* Many independent graphs propagated by one persistent kernel fed from a
- * device work queue, each with its own convergence test. */
+/* Many independent graphs propagated together, each with its own convergence
+ * test and labels (ids local to the graph), bit-exact against running each
+ * graph alone.  opts->batch_mode picks how: LPA_BATCH_LOCKSTEP concatenates
+ * the batch into one graph with shifted ids and runs it through one handle
+ * (any dispatch, the autotuner and the CUDA-graph loop apply), iterating until
+ * every graph has stopped; LPA_BATCH_QUEUE runs one persistent kernel fed
+ * from a device work queue, where a graph leaves as soon as it converges.
+ * Lockstep falls back to the queue when the batch has 2^32 - 1 vertices or
+ * small arcs or more.  The reference runs one graph per process
+ * (src/main.cpp). */
 lpa_status lpa_batch_create(const lpa_graph_desc *graphs, size_t num_graphs, const lpa_opts *o,
                             struct lpa_batch **out);
 lpa_status lpa_batch_run(struct lpa_batch *b, int max_iter, int early_exit, uint32_t *iters_per_graph);
 lpa_status lpa_batch_get_labels(struct lpa_batch *b, size_t graph, uint32_t *host_out, size_t n);
 lpa_status lpa_batch_destroy(struct lpa_batch *b);
+/* The lockstep batch's handle (the concatenated graph), for lpa_autotune,
+ * lpa_set_dispatch, lpa_get_stats and lpa_get_info; NULL in queue mode.  Owned
+ * by the batch.  Its labels are shifted ids: read them with
+ * lpa_batch_get_labels. */
+struct lpa_handle *lpa_batch_handle(struct lpa_batch *b);
 
 #ifdef __cplusplus
 }

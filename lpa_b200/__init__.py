@@ -101,7 +101,13 @@ class Opts(C.Structure):
         ("stream", C.c_void_p),
         ("record_timings", C.c_int),
         ("verbose", C.c_int),
+        ("batch_mode", C.c_int),
     ]
+
+
+class BatchMode(enum.IntEnum):
+    LOCKSTEP = 0  # the batch concatenated into one graph, run by one handle
+    QUEUE = 1  # one persistent launch fed by a device work queue
 
 
 class Info(C.Structure):
@@ -192,6 +198,7 @@ def lib():
     _sig(L, "lpa_hg_csr", [P, u64p, C.POINTER(u64p), C.POINTER(u32p)])
     _sig(L, "lpa_hg_desc", [P, C.POINTER(GraphDesc)])
     _sig(L, "lpa_hg_free", [P])
+    _sig(L, "lpa_hg_concat", [C.POINTER(GraphDesc), C.c_size_t, PP])
     fp = C.POINTER(C.c_float)
     _sig(L, "lpa_mlp_gradient", [C.c_int, fp, fp, u8p, fp, C.c_size_t, fp, fp])
     _sig(L, "lpa_mlp_predict", [C.c_int, fp, fp, C.c_size_t, fp])
@@ -202,6 +209,7 @@ def lib():
     _sig(L, "lpa_batch_run", [P, C.c_int, C.c_int, u32p])
     _sig(L, "lpa_batch_get_labels", [P, C.c_size_t, u32p, C.c_size_t])
     _sig(L, "lpa_batch_destroy", [P])
+    _sig(L, "lpa_batch_handle", [P], C.c_void_p)
     _lib = L
     return L
 
@@ -267,6 +275,18 @@ class HostGraph:
         row = np.ascontiguousarray(row, dtype=np.uint64)
         clm = np.ascontiguousarray(clm, dtype=np.uint32)
         return cls._make(lib().lpa_hg_from_csr, len(row) - 1, _ptr(row, C.c_uint64), _ptr(clm, C.c_uint32))
+
+    @classmethod
+    def concat(cls, graphs):
+        """Compressed graphs as one (lpa_hg_concat): graph k's ids shifted by the
+        vertex counts before it, bitstreams joined bit for bit."""
+        descs = [g.desc() if isinstance(g, HostGraph) else g for g in graphs]
+        arr = (GraphDesc * len(descs))()
+        for i, d in enumerate(descs):
+            C.memmove(C.byref(arr, i * C.sizeof(GraphDesc)), C.byref(d), C.sizeof(GraphDesc))
+        out = C.c_void_p()
+        _check(lib().lpa_hg_concat(arr, len(descs), C.byref(out)), "lpa_hg_concat")
+        return HostGraph(out.value)
 
     @classmethod
     def read_edge_list(cls, path, one_way: bool):
@@ -365,6 +385,9 @@ class Propagator:
         self.n = int(self.info.num_vertices)
 
     def close(self):
+        if getattr(self, "_owner", None) is not None:  # a batch's handle: the batch frees it
+            self._h = None
+            self._owner = None
         if getattr(self, "_h", None):
             lib().lpa_destroy(self._h)
             self._h = None
@@ -510,9 +533,13 @@ def mlp_predict(params, x, device=0):
 
 
 class Batch:
-    """Many graphs propagated together by one persistent launch (lpa_batch_*)."""
+    """Many graphs propagated together, each with its own convergence test
+    (lpa_batch_*).  ``batch_mode`` (BatchMode) picks lockstep, the default, or
+    the persistent queue."""
 
     def __init__(self, graphs, **opts):
+        if "batch_mode" in opts:
+            opts["batch_mode"] = int(opts["batch_mode"])
         descs = [g.desc() if isinstance(g, HostGraph) else g for g in graphs]
         arr = (GraphDesc * len(descs))()
         for i, d in enumerate(descs):
@@ -533,6 +560,20 @@ class Batch:
         out = np.empty(self.n[i], np.uint32)
         _check(lib().lpa_batch_get_labels(self._h, i, _ptr(out, C.c_uint32), self.n[i]), "lpa_batch_get_labels")
         return out
+
+    def handle(self):
+        """The lockstep batch's concatenated graph as a Propagator that the batch
+        owns (autotune, set_dispatch, stats, info); None in queue mode."""
+        h = lib().lpa_batch_handle(self._h)
+        if not h:
+            return None
+        p = Propagator.__new__(Propagator)
+        p._desc = None
+        p._h = C.c_void_p(h)
+        p._owner = self
+        p.info = p.get_info()
+        p.n = int(p.info.num_vertices)
+        return p
 
     def close(self):
         if getattr(self, "_h", None):

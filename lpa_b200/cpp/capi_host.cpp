@@ -1,5 +1,6 @@
 // C ABI of the host format layer (lpa_hg_*): generators, the fast
 // bit-identical CGR encoder and the reference's file formats.
+#include <algorithm>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -227,6 +228,75 @@ lpa_status lpa_hg_desc(lpa_host_graph *g, lpa_graph_desc *d) {
   d->num_small_arcs = c.small_graph.size();
   d->small_offset = c.small_offset.empty() ? nullptr : c.small_offset.data();
   return LPA_OK;
+}
+
+lpa_status lpa_hg_concat(const lpa_graph_desc *graphs, size_t num_graphs, lpa_host_graph **out) {
+  if (!out) return LPA_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!graphs || num_graphs == 0) return LPA_ERR_INVALID_ARG;
+  uint64_t n = 0, n_c = 0, bits = 0, arcs = 0;
+  for (size_t k = 0; k < num_graphs; k++) {
+    const lpa_graph_desc &g = graphs[k];
+    if (g.num_compressed > g.num_vertices || (g.num_vertices && !g.vertices)) return LPA_ERR_INVALID_ARG;
+    if (g.num_compressed && (!g.words || !g.offsets || g.offsets[0] != 0 ||
+                             (g.offsets[g.num_compressed] + 31) / 32 > g.num_words))
+      return LPA_ERR_BAD_STREAM;
+    if (g.num_vertices > g.num_compressed &&
+        (!g.small_offset || g.small_offset[0] != 0 ||
+         g.small_offset[g.num_vertices - g.num_compressed] != g.num_small_arcs || (g.num_small_arcs && !g.small_graph)))
+      return LPA_ERR_INVALID_ARG;
+    n += g.num_vertices;
+    n_c += g.num_compressed;
+    bits += g.num_compressed ? g.offsets[g.num_compressed] : 0;
+    arcs += g.num_vertices > g.num_compressed ? g.num_small_arcs : 0;
+  }
+  // ids and small-CSR offsets are 32-bit
+  if (n > 0xFFFFFFFEull || arcs > 0xFFFFFFFEull) return LPA_ERR_CAPACITY;
+  return guarded([&]() -> lpa_status {
+    auto *h = new lpa_host_graph();
+    lpa::CgrGraph &c = h->cgr;
+    c.n = n;
+    c.n_c = n_c;
+    c.total_bits = bits;
+    c.small_thresh = 0;
+    c.words.assign((bits + 31) / 32 + 4, 0u);  // + the zero tail
+    c.offsets.reserve(n_c + 1);
+    c.vertices.resize(n);
+    c.small_graph.reserve(arcs);
+    if (n > n_c) c.small_offset.reserve(n - n_c + 1);
+    uint64_t at = 0, pc = 0, ps = 0, base = 0;
+    for (size_t k = 0; k < num_graphs; k++) {
+      const lpa_graph_desc &g = graphs[k];
+      const uint64_t gb = g.num_compressed ? g.offsets[g.num_compressed] : 0;
+      // the graph's bits [0, gb) appended at bit `at` (MSB-first words)
+      const uint32_t sh = uint32_t(at & 31);
+      for (uint64_t w = 0; w < (gb + 31) / 32; w++) {
+        uint32_t x = g.words[w];
+        const uint64_t valid = std::min<uint64_t>(32, gb - 32 * w);
+        if (valid < 32) x &= ~0u << (32 - valid);  // bits past the graph's end are not its own
+        const uint64_t dw = at / 32 + w;
+        c.words[dw] |= x >> sh;
+        if (sh) c.words[dw + 1] |= x << (32 - sh);
+      }
+      for (uint64_t i = 0; i < g.num_compressed; i++) c.offsets.push_back(g.offsets[i] + at);
+      for (uint64_t i = 0; i < g.num_compressed; i++) c.vertices[pc + i] = uint32_t(g.vertices[i] + base);
+      for (uint64_t i = g.num_compressed; i < g.num_vertices; i++)
+        c.vertices[n_c + ps + (i - g.num_compressed)] = uint32_t(g.vertices[i] + base);
+      if (g.num_vertices > g.num_compressed) {
+        const uint32_t ab = uint32_t(c.small_graph.size());
+        for (uint64_t i = 0; i < g.num_vertices - g.num_compressed; i++) c.small_offset.push_back(g.small_offset[i] + ab);
+        for (uint64_t e = 0; e < g.num_small_arcs; e++) c.small_graph.push_back(uint32_t(g.small_graph[e] + base));
+      }
+      at += gb;
+      pc += g.num_compressed;
+      ps += g.num_vertices - g.num_compressed;
+      base += g.num_vertices;
+    }
+    c.offsets.push_back(at);
+    if (n > n_c) c.small_offset.push_back(uint32_t(c.small_graph.size()));
+    h->has_cgr = true;
+    return make(out, h);
+  });
 }
 
 lpa_status lpa_hg_free(lpa_host_graph *g) {

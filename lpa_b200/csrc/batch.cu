@@ -1,7 +1,19 @@
-// Batched graphs: many independent graphs propagated by one persistent launch
-// (k_batch) fed by a device ring queue, each graph with its own convergence
-// test.  Graph arrays are packed into one device allocation per kind; every
-// graph keeps its own labels, segments and fixed degree-bucket plan.
+// Batched graphs, each with its own convergence test, in one of two modes.
+//
+// Lockstep (the default): the batch is concatenated into one graph whose
+// vertex ids are shifted per graph, and that graph runs through the ordinary
+// handle (every variant, the learned plan, the autotuner and the CUDA-graph
+// loop) while a two-launch tracker after every iteration records which graphs
+// changed.  Labels are compared, never added, so the shift changes no exact
+// count; the sketch hashes labels relative to their graph's base
+// (IterArgs::gbase), so its counts are those of each graph alone.  A graph
+// that did not change has reached a fixed point: later iterations rewrite
+// the same labels, so its result and iteration count are the ones it has run
+// alone, and the loop ends when every graph has stopped.
+//
+// Queue: one persistent launch (k_batch) fed by a device ring queue; every
+// graph keeps its own labels, segments and fixed degree-bucket plan and
+// leaves the queue as soon as it converges.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,6 +44,9 @@ struct lpa_batch {
   std::vector<unsigned long long> initial_queue;
   uint32_t seeds[kCmsDepth];
   std::string last_error;
+  // lockstep mode: the concatenated graph and each graph's first vertex id
+  lpa_handle *h = nullptr;
+  std::vector<uint32_t> gbase;
 };
 
 namespace {
@@ -53,11 +68,220 @@ void bcheck(cudaError_t e) {
 
 void free_batch(lpa_batch *b) {
   if (!b) return;
+  if (b->h) {
+    lpa_destroy(b->h);
+    delete b;
+    return;
+  }
   if (b->stream) cudaStreamSynchronize(b->stream);
   for (void *p : b->allocs) cudaFree(p);
   if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
   cudaGetLastError();
   delete b;
+}
+
+// ------------------------------------------------------------ lockstep ----
+// The batch as one graph (lpa_hg_concat) and where each graph lies in it.
+struct Union {
+  lpa_host_graph *hg = nullptr;
+  lpa_graph_desc desc{};
+  std::vector<uint32_t> gbase;         // G + 1 vertex-id starts
+  std::vector<uint64_t> cbase, sbase;  // G + 1 compressed / small position starts
+  ~Union() {
+    if (hg) lpa_hg_free(hg);
+  }
+};
+
+// LPA_ERR_CAPACITY when the concatenation's ids leave 32 bits.
+lpa_status build_union(const lpa_graph_desc *graphs, size_t G, Union &u) {
+  lpa_status st = lpa_hg_concat(graphs, G, &u.hg);
+  if (st != LPA_OK) return st;
+  st = lpa_hg_desc(u.hg, &u.desc);
+  if (st != LPA_OK) return st;
+  u.gbase.assign(G + 1, 0);
+  u.cbase.assign(G + 1, 0);
+  u.sbase.assign(G + 1, 0);
+  for (size_t gi = 0; gi < G; gi++) {
+    u.gbase[gi + 1] = u.gbase[gi] + uint32_t(graphs[gi].num_vertices);
+    u.cbase[gi + 1] = u.cbase[gi] + graphs[gi].num_compressed;
+    u.sbase[gi + 1] = u.sbase[gi] + graphs[gi].num_vertices - graphs[gi].num_compressed;
+  }
+  return LPA_OK;
+}
+
+__device__ __forceinline__ uint32_t owner(const uint64_t *base, uint32_t G, uint64_t x) {
+  uint32_t lo = 0, hi = G;  // base[lo] <= x < base[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (base[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Every position's vertex and neighbours lie in its own graph's id range
+// (the handle's own pass checked them against the whole batch only).
+__global__ void k_union_check(DevGraph g, const uint32_t *gbase, const uint64_t *cbase, const uint64_t *sbase,
+                              uint32_t G, uint32_t *err) {
+  for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < g.n; p += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t k = p < g.n_c ? owner(cbase, G, p) : owner(sbase, G, p - g.n_c);
+    const uint32_t lo = gbase[k], hi = gbase[k + 1];
+    const uint32_t node = g.vertices[p];
+    bool bad = node < lo || node >= hi;
+    if (!bad && p < g.n_c) {
+      int64_t iv = 0;
+      walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], node, g.n,
+                      [&](uint32_t v) { bad |= v < lo || v >= hi; }, &iv);
+    } else if (!bad) {
+      for (uint32_t e = g.small_off[p - g.n_c]; e < g.small_off[p - g.n_c + 1]; e++) {
+        const uint32_t v = g.small_nbr[e];
+        bad |= v < lo || v >= hi;
+      }
+    }
+    if (bad) atomicExch(err, 1u);
+  }
+}
+
+// Marks every graph with a vertex whose two label buffers differ: after an
+// iteration these are its changed vertices (vertices without neighbours hold
+// the same label in both).
+__global__ void k_track_changed(const uint32_t *__restrict__ l0, const uint32_t *__restrict__ l1, uint64_t n,
+                                const uint32_t *__restrict__ gbase, uint32_t G, uint32_t *flags) {
+  uint32_t glo = 1, ghi = 0;  // the last owner found: ids [glo, ghi)
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t v0 = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v0 < n; v0 += 4 * stride) {
+    uint32_t a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint64_t v = v0 + u * stride;
+      a[u] = v < n ? __ldcs(l0 + v) : 0u;
+      b[u] = v < n ? __ldcs(l1 + v) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t v = uint32_t(v0 + u * stride);
+      if (a[u] == b[u] || (v >= glo && v < ghi)) continue;  // unchanged, or its graph is marked
+      uint32_t lo = 0, hi = G;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(gbase + mid) <= v) lo = mid;
+        else hi = mid;
+      }
+      glo = __ldg(gbase + lo);
+      ghi = __ldg(gbase + lo + 1);
+      flags[lo] = 1u;
+    }
+  }
+}
+
+// Ends the iteration for the tracker: a running graph whose flag is clear (or
+// that reached max_iter) records the iterations done; flags are cleared.
+__global__ void k_track_step(uint32_t *track, uint32_t G) {
+  __shared__ uint32_t s_it;
+  if (threadIdx.x == 0) s_it = track[0] + 1u;
+  __syncthreads();
+  const uint32_t it = s_it, max_iter = track[1], early = track[2];
+  uint32_t *flags = track + 4, *done = track + 4 + G;
+  for (uint32_t k = threadIdx.x; k < G; k += blockDim.x) {
+    if (done[k] == 0u && ((early && flags[k] == 0u) || it >= max_iter)) done[k] = it;
+    flags[k] = 0u;
+  }
+  if (threadIdx.x == 0) track[0] = it;
+}
+
+}  // namespace
+
+void lpa_rt_enqueue_track(lpa_handle *h) {
+  const int blocks = int(std::max<uint64_t>(1, std::min<uint64_t>((h->n + 1023) / 1024, uint64_t(h->num_sms) * 8)));
+  k_track_changed<<<blocks, 256, 0, h->stream>>>(h->d_lab[0], h->d_lab[1], h->n, h->d_gbase, h->n_graphs,
+                                                 h->d_gtrack + 4);
+  k_track_step<<<1, 1024, 0, h->stream>>>(h->d_gtrack, h->n_graphs);
+}
+
+namespace {
+
+// Lockstep create: the union handle plus the tracker's memory.
+lpa_status create_lockstep(lpa_batch *b, const lpa_graph_desc *graphs, size_t G, const Union &u) {
+  lpa_handle *h = nullptr;
+  lpa_status st = lpa_create(&u.desc, &b->opts, &h);
+  if (st != LPA_OK) return st;
+  b->h = h;
+  b->device = h->device;
+  b->stream = h->stream;
+  b->own_stream = false;
+  auto dev = [&](size_t bytes) -> void * {
+    void *p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(bytes, 4)) != cudaSuccess) {
+      cudaGetLastError();
+      throw LPA_ERR_OOM;
+    }
+    h->allocations.push_back(p);
+    return p;
+  };
+  try {
+    h->d_gbase = static_cast<uint32_t *>(dev((G + 1) * 4));
+    uint64_t *d_cbase = static_cast<uint64_t *>(dev((G + 1) * 8));
+    uint64_t *d_sbase = static_cast<uint64_t *>(dev((G + 1) * 8));
+    h->d_gtrack = static_cast<uint32_t *>(dev((4 + 2 * G) * 4));
+    bcheck(cudaMemcpyAsync(h->d_gbase, u.gbase.data(), (G + 1) * 4, cudaMemcpyHostToDevice, h->stream));
+    bcheck(cudaMemcpyAsync(d_cbase, u.cbase.data(), (G + 1) * 8, cudaMemcpyHostToDevice, h->stream));
+    bcheck(cudaMemcpyAsync(d_sbase, u.sbase.data(), (G + 1) * 8, cudaMemcpyHostToDevice, h->stream));
+    bcheck(cudaMemsetAsync(h->d_gtrack, 0, (4 + 2 * G) * 4, h->stream));
+    bcheck(cudaMemsetAsync(h->d_err, 0, 4, h->stream));
+    DevGraph g;
+    g.words = h->d_words;
+    g.offsets = h->d_offsets;
+    g.vertices = h->d_vertices;
+    g.deg = h->d_deg;
+    g.small_off = h->d_small_off;
+    g.small_nbr = h->d_small_nbr;
+    g.n = h->n;
+    g.n_c = h->n_c;
+    const int blocks = int(std::max<uint64_t>(1, std::min<uint64_t>((h->n + 127) / 128, uint64_t(h->num_sms) * 16)));
+    k_union_check<<<blocks, 128, 0, h->stream>>>(g, h->d_gbase, d_cbase, d_sbase, uint32_t(G), h->d_err);
+    bcheck(cudaGetLastError());
+    uint32_t err = 0;
+    bcheck(cudaMemcpyAsync(&err, h->d_err, 4, cudaMemcpyDeviceToHost, h->stream));
+    bcheck(cudaStreamSynchronize(h->stream));
+    if (err) throw LPA_ERR_BAD_STREAM;
+  } catch (lpa_status e) {
+    return e;
+  }
+  h->n_graphs = uint32_t(G);
+  b->gbase = u.gbase;
+  for (size_t gi = 0; gi < G; gi++) {
+    b->n.push_back(graphs[gi].num_vertices);
+    b->n_c.push_back(graphs[gi].num_compressed);
+  }
+  b->iters.assign(G, 0);
+  return LPA_OK;
+}
+
+lpa_status run_lockstep(lpa_batch *b, int max_iter, int early_exit, uint32_t *iters_per_graph) {
+  lpa_handle *h = b->h;
+  const size_t G = b->gbase.size() - 1;
+  lpa_status st = lpa_init_labels(h);
+  if (st != LPA_OK) return st;
+  try {
+    const uint32_t ctl[4] = {0u, uint32_t(max_iter), early_exit ? 1u : 0u, 0u};
+    bcheck(cudaMemsetAsync(h->d_gtrack, 0, (4 + 2 * G) * 4, h->stream));
+    bcheck(cudaMemcpyAsync(h->d_gtrack, ctl, sizeof(ctl), cudaMemcpyHostToDevice, h->stream));
+  } catch (lpa_status e) {
+    return e;
+  }
+  int done = 0;
+  st = lpa_run(h, max_iter, early_exit, &done);
+  if (st != LPA_OK) return st;
+  std::vector<uint32_t> it(G, 0);
+  if (cudaMemcpyAsync(it.data(), h->d_gtrack + 4 + G, G * 4, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return LPA_ERR_CUDA;
+  }
+  // graphs still marked running ran every iteration of the loop
+  for (size_t gi = 0; gi < G; gi++) b->iters[gi] = it[gi] ? it[gi] : uint32_t(done);
+  if (iters_per_graph) std::memcpy(iters_per_graph, b->iters.data(), G * 4);
+  return LPA_OK;
 }
 
 }  // namespace
@@ -87,6 +311,22 @@ lpa_status lpa_batch_create(const lpa_graph_desc *graphs, size_t num_graphs, con
   lpa_batch *b = new lpa_batch();
   if (o) b->opts = *o;
   else lpa_opts_default(&b->opts);
+  if (b->opts.batch_mode == LPA_BATCH_LOCKSTEP) {
+    Union u;
+    lpa_status st = build_union(graphs, num_graphs, u);
+    if (st == LPA_OK) st = create_lockstep(b, graphs, num_graphs, u);
+    if (st != LPA_ERR_CAPACITY) {  // past 32-bit ids the queue keeps every graph's own ids
+      if (st != LPA_OK) {
+        free_batch(b);
+        return st;
+      }
+      *out = b;
+      return LPA_OK;
+    }
+  } else if (b->opts.batch_mode != LPA_BATCH_QUEUE) {
+    delete b;
+    return LPA_ERR_INVALID_ARG;
+  }
   try {
     if (b->opts.device < 0 || b->opts.device >= count) throw LPA_ERR_INVALID_ARG;
     b->device = b->opts.device;
@@ -239,6 +479,7 @@ lpa_status lpa_batch_create(const lpa_graph_desc *graphs, size_t num_graphs, con
 
 lpa_status lpa_batch_run(lpa_batch *b, int max_iter, int early_exit, uint32_t *iters_per_graph) {
   if (!b || max_iter < 0 || max_iter >= 4096) return LPA_ERR_INVALID_ARG;
+  if (b->h) return run_lockstep(b, max_iter, early_exit, iters_per_graph);
   const size_t G = b->graphs.size();
   try {
     bcheck(cudaSetDevice(b->device));
@@ -308,7 +549,19 @@ lpa_status lpa_batch_run(lpa_batch *b, int max_iter, int early_exit, uint32_t *i
 }
 
 lpa_status lpa_batch_get_labels(lpa_batch *b, size_t graph, uint32_t *host_out, size_t n) {
-  if (!b || graph >= b->graphs.size() || !host_out || n != b->n[graph]) return LPA_ERR_INVALID_ARG;
+  if (!b || graph >= b->n.size() || !host_out || n != b->n[graph]) return LPA_ERR_INVALID_ARG;
+  if (b->h) {
+    lpa_handle *h = b->h;
+    const uint32_t base = b->gbase[graph];
+    if (cudaSetDevice(h->device) != cudaSuccess ||
+        cudaMemcpyAsync(host_out, h->d_lab[h->cur] + base, n * 4, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+      cudaGetLastError();
+      return LPA_ERR_CUDA;
+    }
+    for (size_t i = 0; i < n; i++) host_out[i] -= base;
+    return LPA_OK;
+  }
   const BatchGraph &bg = b->graphs[graph];
   const uint32_t *src = (b->iters[graph] & 1u) ? bg.labs1 : bg.labs0;
   if (cudaSetDevice(b->device) != cudaSuccess ||
@@ -318,6 +571,8 @@ lpa_status lpa_batch_get_labels(lpa_batch *b, size_t graph, uint32_t *host_out, 
   }
   return LPA_OK;
 }
+
+lpa_handle *lpa_batch_handle(lpa_batch *b) { return b ? b->h : nullptr; }
 
 lpa_status lpa_batch_destroy(lpa_batch *b) {
   if (!b) return LPA_ERR_INVALID_ARG;

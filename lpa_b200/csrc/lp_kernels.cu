@@ -129,12 +129,13 @@ struct EpochSink {  // shared epoch table with a running argmax per thread
 struct CmsAddSink {
   uint32_t *cms;
   const uint32_t *seeds;
+  uint32_t base;  // label_base of the vertex
   __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
     const uint32_t w = warp_merge(ok, lab);
     if (w) {
 #pragma unroll
       for (int r = 0; r < kCmsDepth; r++)
-        atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, lab ^ seeds[r]) & (kCmsWidth - 1))], w);
+        atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, (lab - base) ^ seeds[r]) & (kCmsWidth - 1))], w);
     }
   }
 };
@@ -143,13 +144,14 @@ struct CmsAddSink {
 struct CmsBestSink {
   const uint32_t *cms;
   const uint32_t *seeds;
+  uint32_t base;
   uint64_t *best;
   __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
     if (ok) {
       uint32_t est = kFull;
 #pragma unroll
       for (int r = 0; r < kCmsDepth; r++) {
-        const uint32_t v = cms[r * kCmsWidth + (cm_hash(r, lab ^ seeds[r]) & (kCmsWidth - 1))];
+        const uint32_t v = cms[r * kCmsWidth + (cm_hash(r, (lab - base) ^ seeds[r]) & (kCmsWidth - 1))];
         est = v < est ? v : est;
       }
       const uint64_t cand = pack_best(est, lab);
@@ -416,9 +418,10 @@ __device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint3
     uint32_t *cms = tab;
     for (uint32_t i = t; i < kCmsDepth * kCmsWidth; i += kThreads) cms[i] = 0u;
     __syncthreads();
-    const bool staged = heavy_produce(a, c, sh, stage, p, node, d, from_scratch, CmsAddSink{cms, a.seeds});
+    const uint32_t lb = label_base(a, node);
+    const bool staged = heavy_produce(a, c, sh, stage, p, node, d, from_scratch, CmsAddSink{cms, a.seeds, lb});
     __syncthreads();
-    CmsBestSink s2{cms, a.seeds, &best};
+    CmsBestSink s2{cms, a.seeds, lb, &best};
     if (staged) heavy_consume_staged(sh, stage, s2);
     else if ((p >= g.n_c || from_scratch) && d <= kStage) block_consume_stage(stage, d, s2);
     else heavy_produce(a, c, sh, stage, p, node, d, from_scratch, s2);
@@ -908,6 +911,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchArgs b) {
       ia.n_packed = 0;
       ia.gtab = b.gtab;
       ia.gtab_slots = b.gtab_slots;
+      ia.gbase = nullptr;  // every graph has its own labels
+      ia.n_gbase = 0;
     }
     __syncthreads();
     Ctx c;
@@ -1383,11 +1388,12 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
     if (it.kind == kCountSketch) {
       uint32_t *cms = reinterpret_cast<uint32_t *>(cslots);
       for (uint32_t k = t; k < kCmsDepth * kCmsWidth; k += kThreads) cms[k] = 0u;
+      const uint32_t lb = label_base(a, it.node);
       __syncthreads();
       const auto add = [&](uint32_t lab, uint32_t w) {
 #pragma unroll
         for (int r = 0; r < kCmsDepth; r++)
-          atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, lab ^ a.seeds[r]) & (kCmsWidth - 1))], w);
+          atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, (lab - lb) ^ a.seeds[r]) & (kCmsWidth - 1))], w);
       };
       WarpRun run;
       warp_stream<true>(src, d, warp, kWarps, [&](bool ok, uint32_t lab) {
@@ -1410,7 +1416,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
           uint32_t est = kFull;
 #pragma unroll
           for (int r = 0; r < kCmsDepth; r++) {
-            const uint32_t v = cms[r * kCmsWidth + (cm_hash(r, lab ^ a.seeds[r]) & (kCmsWidth - 1))];
+            const uint32_t v = cms[r * kCmsWidth + (cm_hash(r, (lab - lb) ^ a.seeds[r]) & (kCmsWidth - 1))];
             est = v < est ? v : est;
           }
           const uint64_t cand = pack_best(est, lab);

@@ -132,7 +132,25 @@ struct IterArgs {
   // global exact-count tables for exact vertices above kBlockMaxSmemDeg
   uint32_t *gtab;
   uint32_t gtab_slots;          // slots per block (power of two), 0: none
+  // graphs concatenated into one (a lockstep batch): graph k owns the vertex
+  // ids [gbase[k], gbase[k + 1]); n_gbase = 0: one graph
+  const uint32_t *gbase;
+  uint32_t n_gbase;
 };
+
+// The id base of the graph that owns vertex `node`.  The sketch hashes a
+// label relative to it, so a graph's sketch counts are those of the graph run
+// alone; the exact paths compare labels only and need no base.
+__device__ __forceinline__ uint32_t label_base(const IterArgs &a, uint32_t node) {
+  if (a.n_gbase == 0) return 0u;
+  uint32_t lo = 0, hi = a.n_gbase;  // gbase[lo] <= node < gbase[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(a.gbase + mid) <= node) lo = mid;
+    else hi = mid;
+  }
+  return __ldg(a.gbase + lo);
+}
 
 __device__ __forceinline__ uint32_t iter_index(const IterArgs &a) { return a.it_dev ? *a.it_dev : 0u; }
 

@@ -510,6 +510,8 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.scratch_labels = 1;
   a.gtab = h->d_gtab;
   a.gtab_slots = h->gtab_slots;
+  a.gbase = h->d_gbase;
+  a.n_gbase = h->d_gbase ? h->n_graphs : 0u;
   return a;
 }
 
@@ -547,6 +549,10 @@ static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32
     k_iterate<<<h->grid, kThreads, kSmemBytes, h->stream>>>(a);
     h->launches++;
     mark(3);
+  }
+  if (h->d_gtrack) {
+    lpa_rt_enqueue_track(h);
+    h->launches += 2;
   }
   h->ev_used = ne;
   h->cur ^= 1;

@@ -141,6 +141,14 @@ struct lpa_handle {
 
   // learned dispatch (cost model), see dispatch.cu
   struct Learner *learner = nullptr;
+
+  // graphs concatenated into this one (a lockstep batch, batch.cu): graph k
+  // owns vertex ids [d_gbase[k], d_gbase[k + 1]).  d_gtrack: [0] iterations
+  // done, [1] max_iter, [2] early exit, [3] unused, then n_graphs changed
+  // flags, then n_graphs iteration counts (0: still running)
+  uint32_t *d_gbase = nullptr;
+  uint32_t n_graphs = 0;
+  uint32_t *d_gtrack = nullptr;
 };
 
 // Hooks between the runtime modules (C++ linkage).
@@ -153,5 +161,8 @@ void lpa_learner_after_iteration(lpa_handle *h);
 void lpa_learner_stats(lpa_handle *h, lpa_stats *st);
 bool lpa_learner_settled(lpa_handle *h);
 void lpa_rt_enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32_t *work);
+// Per-graph convergence of a lockstep batch, enqueued after every iteration
+// (2 launches).
+void lpa_rt_enqueue_track(lpa_handle *h);
 void lpa_rt_apply_variants(lpa_handle *h);
 lpa_status lpa_rt_take_error(lpa_handle *h);
