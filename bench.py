@@ -51,6 +51,9 @@ WORKLOADS = {
     # [1k, 256k], even graphs road grids (p=0.7), odd graphs R-MAT (edge factor 8),
     # threshold 16, per-graph early exit (the 4096-graph [1k, 2M] batch scaled down)
     "batch-256": dict(kind="batch", graphs=256, n_lo=1000, n_hi=262144, seed=1, small_thresh=16, cms=0, iters=30),
+    # all 4096 graphs, sizes log-uniform in [1k, 128k] (the [1k, 2M] range would hold ~8e9 arcs)
+    "batch-4096": dict(kind="batch", graphs=4096, n_lo=1000, n_hi=131072, seed=1, small_thresh=16, cms=0,
+                       iters=30),
 }
 
 
