@@ -1241,26 +1241,26 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
 
 namespace {
 
-// f(ok, label) for this warp's share of src[0..d): 256-label blocks w,
-// w + nw, ... with 8 loads per lane in flight; warp-synchronous.  keep: the
+// f(ok, label) for this warp's share of src[0..d): 32U-label blocks w,
+// w + nw, ... with U loads per lane in flight; warp-synchronous.  keep: the
 // labels will be read again soon (keep them in L2).
-template <bool keep, class F>
+template <bool keep, int U = 8, class F>
 __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ src, uint32_t d, uint32_t w, uint32_t nw,
                                             F &&f, const uint32_t *__restrict__ labels = nullptr) {
   const uint32_t lane = threadIdx.x & 31u;
-  for (uint32_t b0 = w * 256u; b0 < d; b0 += nw * 256u) {
-    uint32_t v[8];
+  for (uint32_t b0 = w * 32u * U; b0 < d; b0 += nw * 32u * U) {
+    uint32_t v[U];
 #pragma unroll
-    for (int u = 0; u < 8; u++) {
+    for (int u = 0; u < U; u++) {
       const uint32_t k = b0 + 32u * u + lane;
       v[u] = k < d ? (keep ? __ldcg(src + k) : __ldcs(src + k)) : 0u;
     }
     if (labels) {  // src holds ids: gather their labels
 #pragma unroll
-      for (int u = 0; u < 8; u++) v[u] = (b0 + 32u * u + lane < d) ? __ldg(labels + v[u]) : 0u;
+      for (int u = 0; u < U; u++) v[u] = (b0 + 32u * u + lane < d) ? __ldg(labels + v[u]) : 0u;
     }
 #pragma unroll
-    for (int u = 0; u < 8; u++) {
+    for (int u = 0; u < U; u++) {
       const uint32_t k = b0 + 32u * u;
       if (k < d) f(k + lane < d, v[u]);
     }
@@ -1288,8 +1288,10 @@ struct WarpRun {
   }
 };
 
-// Exact counts of this warp's share of src[0..d) into et, with a running
-// argmax in best (the count insert() returns is the label's total so far).
+// Exact counts of this warp's share of src[0..d) (32U-label blocks) into et,
+// with a running argmax in best (the count insert() returns is the label's
+// total so far).
+template <int U = 8>
 __device__ __forceinline__ void count_exact(const EpochTable &et, const uint32_t *__restrict__ src, uint32_t d,
                                             uint32_t w, uint32_t nw, uint64_t &best,
                                             const uint32_t *__restrict__ labels = nullptr) {
@@ -1299,7 +1301,7 @@ __device__ __forceinline__ void count_exact(const EpochTable &et, const uint32_t
     best = cand > best ? cand : best;
   };
   WarpRun run;
-  warp_stream<false>(src, d, w, nw, [&](bool ok, uint32_t lab) {
+  warp_stream<false, U>(src, d, w, nw, [&](bool ok, uint32_t lab) {
     if (run.extend(ok, lab)) return;
     if (run.cnt && lane == 0) ins(run.lab, run.cnt);
     run.restart(ok, lab);
@@ -1307,6 +1309,49 @@ __device__ __forceinline__ void count_exact(const EpochTable &et, const uint32_t
     if (c) ins(lab, c);
   }, labels);
   if (run.cnt && lane == 0) ins(run.lab, run.cnt);
+}
+
+// The sketch of src[0..d) by the whole block in 32U-label blocks: every
+// occurrence added to the zeroed counters cms (a warp-uniform run of one
+// label adds once), then the running argmax of the estimate over the labels
+// in best.
+template <int U>
+__device__ __forceinline__ void sketch_count(uint32_t *cms, const uint32_t *__restrict__ src, uint32_t d, uint32_t lb,
+                                             const uint32_t *seeds, uint64_t &best) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const auto add = [&](uint32_t lab, uint32_t w) {
+#pragma unroll
+    for (int r = 0; r < kCmsDepth; r++)
+      atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, (lab - lb) ^ seeds[r]) & (kCmsWidth - 1))], w);
+  };
+  WarpRun run;
+  warp_stream<true, U>(src, d, warp, kWarps, [&](bool ok, uint32_t lab) {
+    if (run.extend(ok, lab)) return;
+    if (run.cnt && lane == 0) add(run.lab, run.cnt);
+    run.restart(ok, lab);
+    const uint32_t w = warp_merge(ok, lab);
+    if (w) add(lab, w);
+  });
+  if (run.cnt && lane == 0) add(run.lab, run.cnt);
+  __syncthreads();
+  // the estimate depends on the label only: a step whose labels all equal
+  // the label evaluated last adds nothing
+  uint32_t seen = kFull;
+  warp_stream<false, U>(src, d, warp, kWarps, [&](bool ok, uint32_t lab) {
+    const uint32_t okm = __ballot_sync(kFull, ok);
+    if (__ballot_sync(kFull, ok && lab == seen) == okm) return;
+    seen = __shfl_sync(kFull, lab, __ffs(okm) - 1);
+    if (warp_merge(ok, lab)) {
+      uint32_t est = kFull;
+#pragma unroll
+      for (int r = 0; r < kCmsDepth; r++) {
+        const uint32_t v = cms[r * kCmsWidth + (cm_hash(r, (lab - lb) ^ seeds[r]) & (kCmsWidth - 1))];
+        est = v < est ? v : est;
+      }
+      const uint64_t cand = pack_best(est, lab);
+      best = cand > best ? cand : best;
+    }
+  });
 }
 
 // Block-wide maximum of v, returned to every thread.
@@ -1390,45 +1435,17 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
       for (uint32_t k = t; k < kCmsDepth * kCmsWidth; k += kThreads) cms[k] = 0u;
       const uint32_t lb = label_base(a, it.node);
       __syncthreads();
-      const auto add = [&](uint32_t lab, uint32_t w) {
-#pragma unroll
-        for (int r = 0; r < kCmsDepth; r++)
-          atomicAdd(&cms[r * kCmsWidth + (cm_hash(r, (lab - lb) ^ a.seeds[r]) & (kCmsWidth - 1))], w);
-      };
-      WarpRun run;
-      warp_stream<true>(src, d, warp, kWarps, [&](bool ok, uint32_t lab) {
-        if (run.extend(ok, lab)) return;
-        if (run.cnt && lane == 0) add(run.lab, run.cnt);
-        run.restart(ok, lab);
-        const uint32_t w = warp_merge(ok, lab);
-        if (w) add(lab, w);
-      });
-      if (run.cnt && lane == 0) add(run.lab, run.cnt);
-      __syncthreads();
-      // the estimate depends on the label only: a step whose labels all equal
-      // the label evaluated last adds nothing
-      uint32_t seen = kFull;
-      warp_stream<false>(src, d, warp, kWarps, [&](bool ok, uint32_t lab) {
-        const uint32_t okm = __ballot_sync(kFull, ok);
-        if (__ballot_sync(kFull, ok && lab == seen) == okm) return;
-        seen = __shfl_sync(kFull, lab, __ffs(okm) - 1);
-        if (warp_merge(ok, lab)) {
-          uint32_t est = kFull;
-#pragma unroll
-          for (int r = 0; r < kCmsDepth; r++) {
-            const uint32_t v = cms[r * kCmsWidth + (cm_hash(r, (lab - lb) ^ a.seeds[r]) & (kCmsWidth - 1))];
-            est = v < est ? v : est;
-          }
-          const uint64_t cand = pack_best(est, lab);
-          best = cand > best ? cand : best;
-        }
-      });
+      sketch_count<8>(cms, src, d, lb, a.seeds, best);  // smaller blocks gain nothing at degree >= 1024
       best = block_max_u64(best, red);
       // leave no counter behind that a table could read as one of its slots
       for (uint32_t k = t; k < kCmsDepth * kCmsWidth; k += kThreads) cms[k] = 0u;
     } else {
+      // blocks small enough that every warp takes one: the critical path of
+      // a vertex of 512..1024 labels is one block of 64 or 128, not 256
       const EpochTable et{cslots, min(next_pow2(2 * d), kCountBlockSlots), s_epoch};
-      count_exact(et, src, d, warp, kWarps, best);
+      if (d <= 32u * 2u * kWarps) count_exact<2>(et, src, d, warp, kWarps, best);
+      else if (d <= 32u * 4u * kWarps) count_exact<4>(et, src, d, warp, kWarps, best);
+      else count_exact<8>(et, src, d, warp, kWarps, best);
       best = block_max_u64(best, red);
     }
     if (t == 0) {
