@@ -175,14 +175,15 @@ __device__ __forceinline__ int64_t walk_vertex(W w, uint64_t pos, uint64_t end, 
 // with >= 16 leading zeros, zeta with >= 8) are read through win64.
 struct BitReader {
   const uint32_t *__restrict__ w;
-  uint64_t pos;    // absolute position of the next unread bit
   uint64_t buf;    // upcoming bits, MSB-aligned
   uint64_t wnext;  // next word to load into buf
   uint32_t nb;     // valid bits in buf
 
+  // absolute position of the next unread bit (kept implicit: every code
+  // would otherwise pay a 64-bit add)
+  __device__ __forceinline__ uint64_t pos() const { return (wnext << 5) - nb; }
   __device__ __forceinline__ void seek(const uint32_t *__restrict__ words, uint64_t p) {
     w = words;
-    pos = p;
     const uint64_t i = p >> 5;
     const uint32_t s = uint32_t(p) & 31u;
     const uint64_t a = __ldg(w + i), b = __ldg(w + i + 1);
@@ -200,39 +201,41 @@ struct BitReader {
   __device__ __forceinline__ void skip(uint32_t k) {  // k < 64, k <= nb
     buf <<= k;
     nb -= k;
-    pos += k;
   }
+  // After fill() the top 32 bits of buf are valid (nb >= 33); a fast-path
+  // code lies within them, so its fields come from 32-bit shifts.
   __device__ __forceinline__ uint32_t gamma(bool &bad) {
     fill();
-    const uint32_t z = __clzll(buf);
-    if (z < 16) {  // 2z+1 <= 31 bits, and nb >= 33 after fill
+    const uint32_t hi = uint32_t(buf >> 32);
+    const uint32_t z = __clz(hi);
+    if (z < 16) {  // 2z+1 <= 31 bits
       const uint32_t len = 2 * z + 1;
-      const uint32_t v = uint32_t(buf >> (64 - len));
+      const uint32_t v = hi >> (32 - len);
       skip(len);
       return v - 1u;
     }
-    uint64_t p = pos;
+    uint64_t p = pos();
     const uint32_t v = dec_gamma(GWords{w}, p, bad);
     seek(w, p);
     return v;
   }
   __device__ __forceinline__ uint32_t zeta3(bool &bad) {
     fill();
-    const uint32_t h = __clzll(buf);
+    const uint32_t hi = uint32_t(buf >> 32);
+    const uint32_t h = __clz(hi);
     if (h < 8) {  // 4(h+1) <= 32 bits
-      const uint32_t v = uint32_t((buf << (h + 1)) >> (64 - 3 * (h + 1)));
+      const uint32_t v = (hi << (h + 1)) >> (32 - 3 * (h + 1));
       skip(4 * (h + 1));
       return v - 1u;
     }
-    uint64_t p = pos;
+    uint64_t p = pos();
     const uint32_t v = dec_zeta3(GWords{w}, p, bad);
     seek(w, p);
     return v;
   }
   __device__ __forceinline__ uint32_t segcnt(bool &bad) {
     fill();
-    const uint32_t z = __clzll(buf);
-    if (z == 0) {
+    if (buf >> 63) {
       if ((buf >> 62) & 1ull) {
         skip(2);
         return 0;
@@ -254,9 +257,9 @@ __device__ __forceinline__ int64_t walk_vertex_buf(const uint32_t *__restrict__ 
   BitReader r;
   r.seek(words, pos);
   uint32_t nseg = r.segcnt(bad);
-  const uint64_t ibase = r.pos;
-  uint64_t last = r.pos;
-  if (bad || r.pos > end || nseg > (end - r.pos) / kSegBits + 1) return -1;
+  const uint64_t ibase = r.pos();
+  uint64_t last = r.pos();
+  if (bad || r.pos() > end || nseg > (end - r.pos()) / kSegBits + 1) return -1;
   for (uint32_t j = 0; j < nseg; j++) {
     const uint64_t q = ibase + uint64_t(kSegBits) * j;
     if (q >= end) return -1;
@@ -267,19 +270,19 @@ __device__ __forceinline__ int64_t walk_vertex_buf(const uint32_t *__restrict__ 
       const uint32_t l = r.gamma(bad);
       left = (c == 0) ? zigzag_first(node, l) : left + l + 1u;
       const uint32_t len = r.gamma(bad) + kMinItv;
-      if (bad || r.pos > end || uint64_t(left) + len > n) return -1;
+      if (bad || r.pos() > end || uint64_t(left) + len > n) return -1;
       for (uint32_t k = 0; k < len; k++) emit(left + k);
       cnt_all += len;
       left += len;
     }
-    last = r.pos;
+    last = r.pos();
   }
   if (interval_items) *interval_items = cnt_all;
   r.seek(words, last);
   nseg = r.segcnt(bad);
-  const uint64_t rbase = r.pos;
-  last = r.pos;
-  if (bad || r.pos > end || nseg > (end - r.pos) / kSegBits + 1) return -1;
+  const uint64_t rbase = r.pos();
+  last = r.pos();
+  if (bad || r.pos() > end || nseg > (end - r.pos()) / kSegBits + 1) return -1;
   for (uint32_t j = 0; j < nseg; j++) {
     const uint64_t q = rbase + uint64_t(kSegBits) * j;
     if (q >= end) return -1;
@@ -289,11 +292,11 @@ __device__ __forceinline__ int64_t walk_vertex_buf(const uint32_t *__restrict__ 
     for (uint32_t c = 0; c < cnt; c++) {
       const uint32_t x = r.zeta3(bad);
       v = (c == 0) ? zigzag_first(node, x) : v + x + 1u;
-      if (bad || r.pos > end || uint64_t(v) >= n) return -1;
+      if (bad || r.pos() > end || uint64_t(v) >= n) return -1;
       emit(v);
       cnt_all++;
     }
-    last = r.pos;
+    last = r.pos();
   }
   if (bad || last != end) return -1;
   return cnt_all;

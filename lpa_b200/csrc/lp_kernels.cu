@@ -216,13 +216,13 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
     BitReader r;
     r.seek(g.words, g.offsets[p]);
     uint32_t ns = r.segcnt(bad);
-    if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
+    if (bad || r.pos() > end || ns > (end - r.pos()) / kSegBits + 1) {
       bad = true;
       ns = 0;
     }
     sh.nseg_i = ns;
-    sh.ibase = r.pos;
-    sh.last_end = r.pos;
+    sh.ibase = r.pos();
+    sh.last_end = r.pos();
     sh.bad = bad ? 1u : 0u;
     sh.items = 0;
   }
@@ -252,7 +252,7 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
         left = (cc == 0) ? zigzag_first(node, l) : left + l + 1u;
         len = r.gamma(bad) + kMinItv;
         cc++;
-        if (bad || r.pos > end || uint64_t(left) + len > g.n) {
+        if (bad || r.pos() > end || uint64_t(left) + len > g.n) {
           bad = true;
           len = 0;
           cnt = cc;
@@ -285,7 +285,7 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
       }
       __syncthreads();
     }
-    if (has && j == nseg_i - 1) sh.last_end = r.pos;
+    if (has && j == nseg_i - 1) sh.last_end = r.pos();
   }
   __syncthreads();
   // ---- residual section: every warp walks its own 256-bit segments (lane per
@@ -295,13 +295,13 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
     BitReader r;
     r.seek(g.words, sh.last_end);
     uint32_t ns = r.segcnt(bad);
-    if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
+    if (bad || r.pos() > end || ns > (end - r.pos()) / kSegBits + 1) {
       bad = true;
       ns = 0;
     }
     sh.nseg_r = ns;
-    sh.rbase = r.pos;
-    sh.last_end = r.pos;
+    sh.rbase = r.pos();
+    sh.last_end = r.pos();
   }
   __syncthreads();
   const uint32_t nseg_r = sh.nseg_r;
@@ -343,14 +343,14 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
         for (uint32_t cc = 0; cc < cnt; cc++) {
           const uint32_t x = r.zeta3(bad);
           v = (cc == 0) ? zigzag_first(node, x) : v + x + 1u;
-          if (bad || r.pos > end || uint64_t(v) >= g.n) {
+          if (bad || r.pos() > end || uint64_t(v) >= g.n) {
             bad = true;
             v = node;  // keeps the staged id in range; the error word reports the stream
           }
           wst[o++] = v;
         }
         my_items += cnt;
-        if (j == nseg_r - 1) sh.last_end = r.pos;
+        if (j == nseg_r - 1) sh.last_end = r.pos();
       }
       __syncwarp();
       for (uint32_t k0 = lane; k0 < total; k0 += 256) {
@@ -494,9 +494,9 @@ __device__ bool warp_decode_batch(const DevGraph &g, uint32_t *stage, bool activ
     BitReader r;
     r.seek(g.words, g.offsets[p]);
     uint32_t ns = r.segcnt(bad);
-    const uint64_t ib = r.pos;
-    uint64_t last = r.pos;
-    if (bad || r.pos > end || ns > (end - r.pos) / kSegBits + 1) {
+    const uint64_t ib = r.pos();
+    uint64_t last = r.pos();
+    if (bad || r.pos() > end || ns > (end - r.pos()) / kSegBits + 1) {
       bad = true;
       ns = 0;
     }
@@ -513,7 +513,7 @@ __device__ bool warp_decode_batch(const DevGraph &g, uint32_t *stage, bool activ
         const uint32_t l = r.gamma(bad);
         left = (c == 0) ? zigzag_first(node, l) : left + l + 1u;
         const uint32_t len = r.gamma(bad) + kMinItv;
-        if (bad || r.pos > end || uint64_t(left) + len > g.n || uint64_t(itv) + len > d) {
+        if (bad || r.pos() > end || uint64_t(left) + len > g.n || uint64_t(itv) + len > d) {
           bad = true;
           break;
         }
@@ -521,16 +521,16 @@ __device__ bool warp_decode_batch(const DevGraph &g, uint32_t *stage, bool activ
         itv += len;
         left += len;
       }
-      last = r.pos;
+      last = r.pos();
     }
     if (ns) r.seek(g.words, last);
     if (!bad) {
       nres = r.segcnt(bad);
-      rbase = r.pos;
-      if (bad || r.pos > end || nres > (end - r.pos) / kSegBits + 1) {
+      rbase = r.pos();
+      if (bad || r.pos() > end || nres > (end - r.pos()) / kSegBits + 1) {
         bad = true;
         nres = 0;
-      } else if (nres == 0 && r.pos != end) {
+      } else if (nres == 0 && r.pos() != end) {
         bad = true;
       }
     }
@@ -587,13 +587,13 @@ __device__ bool warp_decode_batch(const DevGraph &g, uint32_t *stage, bool activ
       for (uint32_t c = 0; c < cnt; c++) {
         const uint32_t x = rr.zeta3(bad);
         v = (c == 0) ? zigzag_first(ndo, x) : v + x + 1u;
-        if (bad || rr.pos > en || uint64_t(v) >= g.n || rel + c >= dd) {
+        if (bad || rr.pos() > en || uint64_t(v) >= g.n || rel + c >= dd) {
           bad = true;
           break;
         }
         stage[bo + rel + c] = v;
       }
-      if (j == no - 1 && rr.pos != en) bad = true;
+      if (j == no - 1 && rr.pos() != en) bad = true;
     }
     // owners advance by the items of their segments in this round
     const uint32_t fv = (seg_excl > r0 ? seg_excl : r0) - r0;
@@ -1103,7 +1103,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
           for (uint32_t k = 0; k < cnt && !bad; k++) {
             r.gamma(bad);
             items += r.gamma(bad) + kMinItv;
-            if (r.pos > end) bad = true;
+            if (r.pos() > end) bad = true;
           }
         }
       }
@@ -1147,7 +1147,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
         const uint32_t x = r.zeta3(bad);
         v = (done == 0) ? zigzag_first(node, x) : v + x + 1u;
         uint32_t id = v;
-        if (bad || r.pos > end || uint64_t(v) >= g.n) {
+        if (bad || uint64_t(v) >= g.n) {  // the segment's end is checked once, below
           bad = true;
           id = node;  // in range; the error word reports the stream
         }
@@ -1175,6 +1175,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
       }
       __syncwarp();
     }
+    if (ritems && r.pos() > end) bad = true;
     // interval segments: one (left, len) pair per lane per round; the warp
     // expands the round's intervals together (an interval can hold thousands
     // of ids), each lane taking every 32nd id of the concatenation
@@ -1606,18 +1607,18 @@ __global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err) {
     BitReader r;
     r.seek(g.words, o0);
     const uint32_t nsi = r.segcnt(bad);
-    const uint64_t ibase = r.pos;
-    uint64_t last = r.pos;
+    const uint64_t ibase = r.pos();
+    uint64_t last = r.pos();
     if (!bad && nsi && ibase + uint64_t(kSegBits) * (nsi - 1) < end) {
       // only the last interval segment is unpadded: decode it to find its end
       BitReader q;
       q.seek(g.words, ibase + uint64_t(kSegBits) * (nsi - 1));
       const uint32_t cnt = q.gamma(bad);
-      for (uint32_t k = 0; k < cnt && !bad && q.pos <= end; k++) {
+      for (uint32_t k = 0; k < cnt && !bad && q.pos() <= end; k++) {
         q.gamma(bad);
         q.gamma(bad);
       }
-      last = q.pos;
+      last = q.pos();
     } else if (nsi) {
       bad = true;
     }
@@ -1626,7 +1627,7 @@ __global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err) {
     if (!bad && last <= end) {
       r.seek(g.words, last);
       nsr = r.segcnt(bad);
-      rbase = r.pos;
+      rbase = r.pos();
     }
     if (bad || rbase > end || rbase - o0 > 0xFFFFFFFFull || (nsr && rbase + uint64_t(kSegBits) * (nsr - 1) >= end)) {
       set_error(err, kErrBadStream);
