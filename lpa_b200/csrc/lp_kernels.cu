@@ -1161,7 +1161,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           const uint32_t f = f0 + 32u * u + lane;
-          lv[u] = f < w1 ? ld_label(c, wst[f - w0]) : 0u;
+          lv[u] = f < w1 ? __ldcg(c.lab_in + wst[f - w0]) : 0u;  // random: L2 only, L1 keeps the stream
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {

@@ -49,7 +49,7 @@ struct WorkItem {
 struct DecodeGroup {
   uint32_t p0, j0, nlanes, seg;
 };
-constexpr uint32_t kDecodeWindow = 1024;  // staged ids per warp of the pre-pass
+constexpr uint32_t kDecodeWindow = 768;  // staged ids per warp of the pre-pass
 
 // Work of the two-pass count pass (k_count_two_pass): positions p0 ..
 // p0 + np - 1, all of one kind, whose labels the pre-pass wrote to the
