@@ -181,6 +181,8 @@ typedef struct lpa_tune {
   uint32_t warp_positions;   /* vertices per one-vertex-at-a-time warp item, 1..32; default 4 */
   uint32_t warp_max_degree;  /* largest degree one warp counts (32..511); a block counts larger; default 511 */
   uint32_t warp_claim;       /* warp items a warp claims from the queue at once, 1..8; default 2 */
+  uint32_t bulk_stage;       /* 1: several-vertices warp items stage their labels with one bulk copy
+                                (cp.async.bulk into shared memory) instead of per-lane loads; default 0 */
 } lpa_tune;
 lpa_status lpa_get_tune(struct lpa_handle *h, lpa_tune *out);
 /* Installs the knobs (out of range: LPA_ERR_INVALID_ARG) and rebuilds the work lists. */

@@ -71,10 +71,11 @@ class Tune(C.Structure):
         ("warp_positions", C.c_uint32),
         ("warp_max_degree", C.c_uint32),
         ("warp_claim", C.c_uint32),
+        ("bulk_stage", C.c_uint32),
     ]
 
     def as_tuple(self):
-        return (self.group_positions, self.warp_positions, self.warp_max_degree, self.warp_claim)
+        return (self.group_positions, self.warp_positions, self.warp_max_degree, self.warp_claim, self.bulk_stage)
 
 
 class GraphDesc(C.Structure):
@@ -472,8 +473,8 @@ class Propagator:
         self._chk(lib().lpa_get_tune(self._h, C.byref(t)), "lpa_get_tune")
         return t
 
-    def set_tune(self, group_positions, warp_positions, warp_max_degree, warp_claim):
-        t = Tune(group_positions, warp_positions, warp_max_degree, warp_claim)
+    def set_tune(self, group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage=0):
+        t = Tune(group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage)
         self._chk(lib().lpa_set_tune(self._h, C.byref(t)), "lpa_set_tune")
 
     def autotune(self, cache_path=None, repeats=2) -> Tune:

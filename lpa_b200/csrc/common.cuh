@@ -173,6 +173,50 @@ __device__ __forceinline__ int64_t walk_vertex(W w, uint64_t pos, uint64_t end, 
 // Sequential MSB-first reader with a 64-bit register buffer: one 32-bit load
 // per 32 bits consumed.  Codes that do not fit the buffer's fast path (gamma
 // with >= 16 leading zeros, zeta with >= 8) are read through win64.
+// ---------------------------------------------------------- bulk copies ---
+// 1-D bulk copies global -> shared memory by the copy engine
+// (cp.async.bulk, sm_90+), completed on an mbarrier in shared memory.  Never
+// with cluster multicast.  Source and destination 16-byte aligned, size a
+// multiple of 16.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return uint32_t(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// makes initialised mbarriers visible to the copy engine
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// orders this thread's earlier generic accesses to shared memory before
+// later bulk-copy writes to it
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// one arrival that also expects `bytes` of copies to complete on bar, then
+// the copy itself
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0u;
+}
+// Waits for phase `parity` of bar to complete, giving up after `limit` tries
+// (each try suspends the thread for a bounded time).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
+  for (uint32_t i = 0; i < limit; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
 struct BitReader {
   const uint32_t *__restrict__ w;
   uint64_t buf;    // upcoming bits, MSB-aligned

@@ -1380,9 +1380,11 @@ __device__ __forceinline__ uint64_t block_max_u64(uint64_t v, uint64_t *red) {
 // groups.  The same shared memory serves the warp tables, the block table
 // (block epochs, disjoint from the warps') and the sketch (cleared before and
 // after use).  Every position's pre-pass cursor is reset here.
+template <bool kBulk>
 __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
-  extern __shared__ unsigned long long cslots[];
+  extern __shared__ __align__(128) unsigned long long cslots[];
   __shared__ uint64_t red[kWarps];
+  __shared__ uint64_t s_bar[kWarps];  // per warp: completion of its bulk copies
   __shared__ uint32_t s_has, s_epoch;
   __shared__ BlockItem s_bi;
   const DevGraph &g = a.g;
@@ -1391,6 +1393,8 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
   const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
   for (uint32_t i = t; i < kCountBlockSlots; i += kThreads) cslots[i] = 0ull;
   if (t == 0) s_epoch = kHeavyEpochFirst;
+  if (lane == 0) mbar_init(s_bar + warp, 1u);
+  fence_mbar_init();
   __syncthreads();
   uint32_t *qctr = a.work + 4 * (a.it_dev ? c.it : 0u) + 2;
   unsigned long long changed = 0;
@@ -1469,7 +1473,9 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
 
   unsigned long long *wslots = cslots + warp * kCountWarpSlots;
   uint32_t wepoch = 0;
-  for (;;) {
+  uint32_t bphase = 0;  // parity of this warp's next bulk-copy phase
+  bool stop = false;    // a bulk copy did not complete in time
+  while (!stop) {
     uint32_t i0 = 0;
     const uint32_t claim = a.warp_claim ? a.warp_claim : 2u;
     if (lane == 0) i0 = atomicAdd(qctr + 1, claim);
@@ -1498,27 +1504,48 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
         const uint64_t ao0 = (uint64_t(__shfl_sync(kFull, uint32_t(ao >> 32), 0)) << 32) |
                              __shfl_sync(kFull, uint32_t(ao), 0);
         uint32_t *wstage = reinterpret_cast<uint32_t *>(wslots);
-        for (uint32_t k0 = 0; k0 < total; k0 += 256) {
-          uint32_t v[8];
-#pragma unroll
-          for (int u = 0; u < 8; u++) {
-            const uint32_t kk = k0 + 32u * u + lane;
-            v[u] = kk >= total ? 0u : (ids ? __ldg(g.small_nbr + ao0 + kk) : __ldcs(a.scratch + ao0 + kk));
+        // scratch labels: one bulk copy of the 16-byte-aligned bytes around
+        // the range (the scratch is padded at its end), the labels then at
+        // wstage[sh0..); the small CSR gathers ids
+        const uint64_t b_lo = (ao0 * 4u) & ~15ull, b_hi = ((ao0 + total) * 4u + 15u) & ~15ull;
+        const bool bulk = kBulk && !ids && total >= kBulkMinLabels && b_hi - b_lo <= kCountWarpSlots * 8u;
+        const uint32_t sh0 = bulk ? uint32_t(ao0 & 3u) : 0u;
+        if (bulk) {
+          fence_proxy_async_smem();  // this lane's earlier accesses to wstage come first
+          __syncwarp();
+          if (lane == 0)
+            bulk_load(wstage, reinterpret_cast<const char *>(a.scratch) + b_lo, uint32_t(b_hi - b_lo), s_bar + warp);
+          if (!__all_sync(kFull, mbar_wait(s_bar + warp, bphase, kBulkWaitTries))) {
+            if (lane == 0) set_error(a.err, kErrTimeout);
+            mbar_wait(s_bar + warp, bphase, kBulkWaitTries);  // the copy still writes wstage
+            stop = true;
+            break;
           }
-          if (ids) {
+          bphase ^= 1u;
+        } else {
+          for (uint32_t k0 = 0; k0 < total; k0 += 256) {
+            uint32_t v[8];
 #pragma unroll
-            for (int u = 0; u < 8; u++) v[u] = (k0 + 32u * u + lane < total) ? ld_label(c, v[u]) : 0u;
+            for (int u = 0; u < 8; u++) {
+              const uint32_t kk = k0 + 32u * u + lane;
+              v[u] = kk >= total ? 0u : (ids ? __ldg(g.small_nbr + ao0 + kk) : __ldcs(a.scratch + ao0 + kk));
+            }
+            if (ids) {
+#pragma unroll
+              for (int u = 0; u < 8; u++) v[u] = (k0 + 32u * u + lane < total) ? ld_label(c, v[u]) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+              if (k0 + 32u * u + lane < total) wstage[k0 + 32u * u + lane] = v[u];
           }
-#pragma unroll
-          for (int u = 0; u < 8; u++)
-            if (k0 + 32u * u + lane < total) wstage[k0 + 32u * u + lane] = v[u];
         }
         __syncwarp();
+        const uint32_t *lbl = wstage + sh0;
         // a vertex whose labels are all equal takes that label: lane v checks
         // its own vertex; only the others are counted below
         bool mixed = false;
-        const uint32_t first = (lane < it.np && d) ? wstage[excl] : 0u;
-        for (uint32_t j = 1; j < d; j++) mixed |= wstage[excl + j] != first;
+        const uint32_t first = (lane < it.np && d) ? lbl[excl] : 0u;
+        for (uint32_t j = 1; j < d; j++) mixed |= lbl[excl + j] != first;
         if (lane < it.np && d && !mixed) {  // an isolated vertex keeps its label in both buffers
           c.lab_out[node] = first;
           my_changed += (first != old);
@@ -1540,7 +1567,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
             const uint32_t oldv = __shfl_sync(kFull, old, srcl);
             const uint32_t ev = __shfl_sync(kFull, excl, srcl);
             const bool ok = vin && k < dv;
-            const uint32_t lab = ok ? wstage[ev + k] : kFull;
+            const uint32_t lab = ok ? lbl[ev + k] : kFull;
             const uint32_t cnt = group_counts(ok, lab, gm, gl);
             const uint32_t maxc = __reduce_max_sync(gm, cnt);
             const uint32_t bestl = __reduce_min_sync(gm, (ok && cnt == maxc) ? lab : kFull);
@@ -1552,7 +1579,8 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
         }
         __syncwarp();
         // the staged labels must not read as table slots later
-        for (uint32_t k2 = lane; k2 < (total + 1) / 2; k2 += 32) wslots[k2] = 0ull;
+        const uint32_t used = bulk ? uint32_t(b_hi - b_lo) / 8u : (total + 1) / 2;
+        for (uint32_t k2 = lane; k2 < used; k2 += 32) wslots[k2] = 0ull;
         __syncwarp();
       } else {
         // every vertex's metadata in one round of loads (lane j: vertex j)
@@ -1598,6 +1626,9 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
   busy_mark(a, 1, true);
   flush_changed(c.changed, changed);
 }
+
+template __global__ void k_count_two_pass<false>(IterArgs a);
+template __global__ void k_count_two_pass<true>(IterArgs a);
 
 __global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err) {
   for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < g.n_c;

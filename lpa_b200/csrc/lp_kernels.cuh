@@ -72,6 +72,11 @@ struct BlockItem {
 constexpr uint32_t kCountWarpSlots = 512;
 constexpr uint32_t kCountWarpMax = kCountWarpSlots - 1;  // tables fill up to load 1 (triangular probing)
 constexpr uint32_t kCountBlockSlots = kWarps * kCountWarpSlots;  // the warps' tables together
+// with lpa_tune.bulk_stage, group items of the count pass with at least this
+// many scratch labels are staged by one bulk copy (cp.async.bulk) instead of
+// per-lane loads
+constexpr uint32_t kBulkMinLabels = 64;
+constexpr uint32_t kBulkWaitTries = 1u << 22;  // mbarrier try_wait attempts before a copy counts as lost
 constexpr uint32_t kCountBlockMax = 2047;
 constexpr uint32_t kCountSmemBytes = kCountBlockSlots * 8;        // 32 KB
 
@@ -194,6 +199,8 @@ __global__ void k_decode_two_pass(IterArgs a);
 // V2 for tiny vertices: a lane per vertex.
 __global__ void k_packed(IterArgs a);
 // Two-pass variant, pass 2: counts the labels the pre-pass wrote.
+// kBulk: group items staged by bulk copies (lpa_tune.bulk_stage)
+template <bool kBulk>
 __global__ void k_count_two_pass(IterArgs a);
 
 struct DecodeArgs {

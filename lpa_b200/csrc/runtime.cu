@@ -365,7 +365,8 @@ static void ensure_two_pass_scratch(lpa_handle *h) {
   for (uint64_t p = 0; p < h->n; p++) off[p + 1] = off[p] + h->h_deg[p];
   h->d_arc_off = dalloc<uint64_t>(h, h->n + 1, "arc offsets");
   h2d(h, h->d_arc_off, off.data(), h->n + 1, "upload arc offsets");
-  h->d_scratch = dalloc<uint32_t>(h, off[h->n_c], "two-pass scratch");
+  // + 4: a 16-byte-aligned bulk copy may read up to 12 bytes past the last label
+  h->d_scratch = dalloc<uint32_t>(h, off[h->n_c] + 4, "two-pass scratch");
   // where every compressed position's segments start, for the pre-pass
   const uint64_t nc = std::max<uint64_t>(1, h->n_c);
   h->d_pidx = dalloc<uint4>(h, nc, "position index");
@@ -536,7 +537,8 @@ static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32
     mark(0);
   }
   if (h->n_cblock + h->n_cwarp) {
-    k_count_two_pass<<<h->grid_count, kThreads, kCountSmemBytes, h->stream>>>(a);
+    if (h->tune.bulk_stage) k_count_two_pass<true><<<h->grid_count, kThreads, kCountSmemBytes, h->stream>>>(a);
+    else k_count_two_pass<false><<<h->grid_count, kThreads, kCountSmemBytes, h->stream>>>(a);
     h->launches++;
     mark(1);
   }
@@ -659,9 +661,14 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ, k_iterate, kThreads, kSmemBytes), "occupancy");
     h->occ = std::max(1, h->occ);
     h->grid = h->num_sms * h->occ;
-    int occ_count = 1;
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_count, k_count_two_pass, kThreads, kCountSmemBytes),
+    int occ_count = 1, occ_bulk = 1;
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_count, k_count_two_pass<false>, kThreads,
+                                                           kCountSmemBytes),
           "occupancy");
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_bulk, k_count_two_pass<true>, kThreads,
+                                                           kCountSmemBytes),
+          "occupancy");
+    occ_count = std::min(occ_count, occ_bulk);  // one grid for both forms
     h->grid_count = h->num_sms * std::max(1, occ_count);
     int occ_decode = 1;
     check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_decode, k_decode_two_pass, kThreads, 0), "occupancy");
@@ -960,7 +967,8 @@ lpa_status lpa_set_dispatch(lpa_handle *h, int dispatch, int force_variant) {
 
 static bool tune_valid(const lpa_tune &t) {
   return t.group_positions >= 1 && t.group_positions <= 32 && t.warp_positions >= 1 && t.warp_positions <= 32 &&
-         t.warp_max_degree >= 32 && t.warp_max_degree <= kCountWarpMax && t.warp_claim >= 1 && t.warp_claim <= 8;
+         t.warp_max_degree >= 32 && t.warp_max_degree <= kCountWarpMax && t.warp_claim >= 1 && t.warp_claim <= 8 &&
+         t.bulk_stage <= 1;
 }
 
 // One iteration from the current labels, repeated; the labels are left as
@@ -1007,7 +1015,7 @@ static std::string tune_key(const lpa_handle *h) {
   uint64_t arcs = 0;
   for (const auto &sg : h->segs) arcs += sg.arcs;
   char buf[512];
-  std::snprintf(buf, sizeof(buf), "%s|sm%d|n%llu|nc%llu|arcs%llu|cms%u|plan%016llx", gpu.c_str(), pr.multiProcessorCount,
+  std::snprintf(buf, sizeof(buf), "v2|%s|sm%d|n%llu|nc%llu|arcs%llu|cms%u|plan%016llx", gpu.c_str(), pr.multiProcessorCount,
                 (unsigned long long)h->n, (unsigned long long)h->n_c, (unsigned long long)arcs,
                 h->opts.cms_threshold, (unsigned long long)fnv);
   return buf;
@@ -1045,8 +1053,8 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
         std::istringstream ls(line);
         std::string k;
         lpa_tune t{};
-        if (ls >> k >> t.group_positions >> t.warp_positions >> t.warp_max_degree >> t.warp_claim && k == key &&
-            tune_valid(t)) {
+        if (ls >> k >> t.group_positions >> t.warp_positions >> t.warp_max_degree >> t.warp_claim >> t.bulk_stage &&
+            k == key && tune_valid(t)) {
           h->tune = t;
           found = true;
         }
@@ -1060,17 +1068,18 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
       double best_ms = tune_trial(h, repeats);
       if (best_ms < 0) throw Fail{LPA_ERR_CUDA, "autotune: " + h->last_error};
       static const uint32_t groups[] = {8, 16, 24, 32}, warps[] = {1, 2, 4, 8, 16},
-                            degs[] = {63, 127, 255, kCountWarpMax}, claims[] = {1, 2, 4, 8};
+                            degs[] = {63, 127, 255, kCountWarpMax}, claims[] = {1, 2, 4, 8}, bulks[] = {0, 1};
       for (int sweep = 0; sweep < 2; sweep++) {
-        for (int knob = 0; knob < 4; knob++) {
-          const uint32_t *vals = knob == 0 ? groups : knob == 1 ? warps : knob == 2 ? degs : claims;
-          const int nv = knob == 1 ? 5 : 4;
+        for (int knob = 0; knob < 5; knob++) {
+          const uint32_t *vals = knob == 0 ? groups : knob == 1 ? warps : knob == 2 ? degs : knob == 3 ? claims : bulks;
+          const int nv = knob == 1 ? 5 : knob == 4 ? 2 : 4;
           for (int i = 0; i < nv; i++) {
             lpa_tune cand = best;
             uint32_t &slot = knob == 0 ? cand.group_positions
                              : knob == 1 ? cand.warp_positions
                              : knob == 2 ? cand.warp_max_degree
-                                         : cand.warp_claim;
+                             : knob == 3 ? cand.warp_claim
+                                         : cand.bulk_stage;
             if (slot == vals[i]) continue;
             slot = vals[i];
             h->tune = cand;
@@ -1089,7 +1098,7 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
       if (cache_path) {
         std::ofstream o(cache_path, std::ios::app);
         o << key << ' ' << best.group_positions << ' ' << best.warp_positions << ' ' << best.warp_max_degree << ' '
-          << best.warp_claim << ' ' << best_ms << '\n';
+          << best.warp_claim << ' ' << best.bulk_stage << ' ' << best_ms << '\n';
       }
     }
     if (out) *out = h->tune;

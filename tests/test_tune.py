@@ -21,8 +21,9 @@ def _two_pass(p):
     p.set_plan(plan)
 
 
-@pytest.mark.parametrize("knobs", [(1, 1, 32, 1), (7, 3, 100, 8), (32, 32, 511, 5)])
+@pytest.mark.parametrize("knobs", [(1, 1, 32, 1, 0), (7, 3, 100, 8, 1), (32, 32, 511, 5, 0), (32, 4, 511, 2, 1)])
 def test_knobs_keep_labels_exact(knobs):
+    """bulk_stage = 1 stages the several-vertices items by bulk copies."""
     g, ref = _load("rmat_t16")
     hist, changed = oracle.lp_run(ref["row"], ref["clm"], 4, 64)
     with L.Propagator(g, cms_threshold=64) as p:
@@ -38,7 +39,8 @@ def test_out_of_range_knobs_are_refused():
     g, _ = _load("road_a")
     with L.Propagator(g) as p:
         before = p.get_tune().as_tuple()
-        for bad in [(0, 4, 511, 2), (33, 4, 511, 2), (32, 4, 31, 2), (32, 4, 512, 2), (32, 4, 511, 9)]:
+        for bad in [(0, 4, 511, 2), (33, 4, 511, 2), (32, 4, 31, 2), (32, 4, 512, 2), (32, 4, 511, 9),
+                    (32, 4, 511, 2, 2)]:
             with pytest.raises(L.LpaError) as e:
                 p.set_tune(*bad)
             assert e.value.status == L.Status.INVALID_ARG
@@ -66,3 +68,18 @@ def test_autotune_leaves_labels_and_caches(tmp_path):
             _two_pass(q)
             assert q.autotune(cache).as_tuple() == t.as_tuple()
         assert cache.read_text().count("\n") == 1
+
+
+@pytest.mark.parametrize("case,thr", [("road_a", 0), ("copy_t16", 0), ("stress_t8", 8)])
+def test_bulk_staged_groups_exact(case, thr):
+    """Several-vertices items staged by one bulk copy each (16-byte-aligned
+    ranges around arbitrary scratch offsets) give the oracle's labels."""
+    g, ref = _load(case)
+    hist, changed = oracle.lp_run(ref["row"], ref["clm"], 3, thr)
+    with L.Propagator(g, cms_threshold=thr) as p:
+        _two_pass(p)
+        t = p.get_tune().as_tuple()
+        p.set_tune(*t[:4], 1)
+        for it in range(3):
+            assert p.iterate() == changed[it]
+            assert np.array_equal(p.labels(), hist[it]), f"iteration {it + 1}"
