@@ -147,6 +147,9 @@ def run_batch(args, w, rank, world, local):
             degs.append(int(row[-1]))
         for _ in range(args.warmup):
             iters = bt.run(w["iters"], early_exit=True)
+        tune = None
+        if h is not None and args.autotune:  # tuned on the labels the last warm-up run left
+            tune = list(h.autotune(None, repeats=2).as_tuple())
         barrier(world, device)
         torch.cuda.synchronize()
         launches0 = h.stats().launches if h is not None else 0
@@ -194,7 +197,7 @@ def run_batch(args, w, rank, world, local):
                            "arcs": int(sum(degs)), "iterations_per_graph": [int(k) for k in iters][:8] + ["..."],
                            "l2": "inputs larger than L2" if sum(algorithmic_bytes(a) for a in arrs) > 2 * L2_BYTES
                            else "resident", "parallelism": f"replicas x{world}", "batch_mode": args.batch_mode,
-                           "dispatch": args.dispatch if h is not None else "fixed"},
+                           "dispatch": args.dispatch if h is not None else "fixed", "tune": tune},
                 "roofline": {"bound": "hbm", "kernel": "lockstep iteration kernels" if h is not None else "k_batch",
                              "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": peak_kind, "traffic": None},
@@ -350,6 +353,10 @@ def main():
     ap.add_argument("--dispatch", default="learned", choices=["fixed", "learned"],
                     help="learned: the MLP plan (judged against the fixed buckets, also measured)")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--tune", default="",
+                    help="explicit two-pass knobs g,w,d,c,bulk,l2 (lpa_tune), instead of the autotuner")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip tuning the count pass's work shapes (lpa_autotune) after the learner's warm-up")
     ap.add_argument("--batch-mode", default="lockstep", choices=["lockstep", "queue"],
                     help="batched workloads: the concatenated graph in lockstep, or the persistent queue")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -423,15 +430,23 @@ def main():
     if args.dispatch == "learned":
         # the cost model explores and trains on warm-up iterations, then its plan is timed
         p.set_dispatch(L.Dispatch.LEARNED)
+        tune = None
+        if args.tune:  # explicit knobs: no tuning
+            p.set_tune(*[int(x) for x in args.tune.split(",")])
+            tune = list(p.get_tune().as_tuple())
         p.init_labels()
         for _ in range(max(args.warmup, 8)):
             p.iterate()
+        if args.autotune and not args.tune:  # the two-pass knobs, tuned on these mid-run labels
+            tune = list(p.autotune(None, repeats=2).as_tuple())
         p.init_labels()
         ls = p.stats()
         learned_info = {"active": int(ls.learned_active), "mlp_updates": int(ls.mlp_updates),
                         "mlp_loss": float(ls.mlp_loss), "reverts": int(ls.dispatch_reverts),
                         "segments_per_variant": [int(x) for x in ls.variant_segments],
-                        "arcs_per_variant": [int(x) for x in ls.variant_arcs]}
+                        "arcs_per_variant": [int(x) for x in ls.variant_arcs],
+                        "tune": tune if tune is not None else list(p.get_tune().as_tuple()),
+                        "autotuned": tune is not None and not args.tune}
 
     st0 = p.stats()
     barrier(world, device)

@@ -174,7 +174,7 @@ lpa_status lpa_set_dispatch(struct lpa_handle *h, int dispatch, int force_varian
  * (baselines/novaplus/novaplus_propogator.cuh:219-220). */
 lpa_status lpa_set_plan(struct lpa_handle *h, const uint8_t *variant, size_t count);
 
-/* Work shapes of the two-pass count pass: the autotuner's knobs.  No
+/* Work shapes and cache policies of the two-pass kernels: the autotuner's knobs.  No
  * counterpart in the reference, whose shapes are compile-time constants. */
 typedef struct lpa_tune {
   uint32_t group_positions;  /* positions (degree <= 32) per several-vertices warp item, 1..32; default 32 */
@@ -183,6 +183,9 @@ typedef struct lpa_tune {
   uint32_t warp_claim;       /* warp items a warp claims from the queue at once, 1..8; default 2 */
   uint32_t bulk_stage;       /* 1: several-vertices warp items stage their labels with one bulk copy
                                 (cp.async.bulk into shared memory) instead of per-lane loads; default 0 */
+  uint32_t l2_gathers;       /* 1: the two-pass pre-pass reads residual labels through L2 only, leaving L1
+                                to the bitstream; 0: through L1, which pays when hot labels take many
+                                reads; default 0 */
 } lpa_tune;
 lpa_status lpa_get_tune(struct lpa_handle *h, lpa_tune *out);
 /* Installs the knobs (out of range: LPA_ERR_INVALID_ARG) and rebuilds the work lists. */

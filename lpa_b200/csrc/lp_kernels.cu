@@ -1049,6 +1049,10 @@ __global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
 // segment counts and a 5-step search; the lanes of one position reserve their
 // output range with one atomicAdd on the position's cursor, since the labels
 // of a position may sit in any order.  No block barriers: warps run alone.
+// kL2Gather: residual labels are read through L2 only (ld.global.cg), leaving
+// L1 to the bitstream; without it they go through L1, which pays when a few
+// hot labels take many of the reads (lpa_tune.l2_gathers).
+template <bool kL2Gather>
 __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   __shared__ uint32_t stage[kWarps * kDecodeWindow];
   __shared__ uint8_t owner[kWarps * kDecodeWindow];
@@ -1161,7 +1165,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           const uint32_t f = f0 + 32u * u + lane;
-          lv[u] = f < w1 ? __ldcg(c.lab_in + wst[f - w0]) : 0u;  // random: L2 only, L1 keeps the stream
+          lv[u] = f < w1 ? (kL2Gather ? __ldcg(c.lab_in + wst[f - w0]) : ld_label(c, wst[f - w0])) : 0u;
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {
@@ -1239,6 +1243,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   }
   busy_mark(a, 0, true);
 }
+
+template __global__ void k_decode_two_pass<false>(IterArgs a);
+template __global__ void k_decode_two_pass<true>(IterArgs a);
 
 namespace {
 
