@@ -183,9 +183,9 @@ typedef struct lpa_tune {
   uint32_t warp_claim;       /* warp items a warp claims from the queue at once, 1..8; default 2 */
   uint32_t bulk_stage;       /* 1: several-vertices warp items stage their labels with one bulk copy
                                 (cp.async.bulk into shared memory) instead of per-lane loads; default 0 */
-  uint32_t l2_gathers;       /* 1: the two-pass pre-pass reads residual labels through L2 only, leaving L1
-                                to the bitstream; 0: through L1, which pays when hot labels take many
-                                reads; default 0 */
+  uint32_t gather_cache;     /* cache path of the two-pass pre-pass's label reads: 0 (default) the labels
+                                of the lowest n/64 ids through L1, the rest through L2 only; 1 all through
+                                L2 only, leaving L1 to the bitstream; 2 all through L1 (hot labels) */
 } lpa_tune;
 lpa_status lpa_get_tune(struct lpa_handle *h, lpa_tune *out);
 /* Installs the knobs (out of range: LPA_ERR_INVALID_ARG) and rebuilds the work lists. */

@@ -72,12 +72,12 @@ class Tune(C.Structure):
         ("warp_max_degree", C.c_uint32),
         ("warp_claim", C.c_uint32),
         ("bulk_stage", C.c_uint32),
-        ("l2_gathers", C.c_uint32),
+        ("gather_cache", C.c_uint32),
     ]
 
     def as_tuple(self):
         return (self.group_positions, self.warp_positions, self.warp_max_degree, self.warp_claim, self.bulk_stage,
-                self.l2_gathers)
+                self.gather_cache)
 
 
 class GraphDesc(C.Structure):
@@ -475,8 +475,8 @@ class Propagator:
         self._chk(lib().lpa_get_tune(self._h, C.byref(t)), "lpa_get_tune")
         return t
 
-    def set_tune(self, group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage=0, l2_gathers=0):
-        t = Tune(group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage, l2_gathers)
+    def set_tune(self, group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage=0, gather_cache=0):
+        t = Tune(group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage, gather_cache)
         self._chk(lib().lpa_set_tune(self._h, C.byref(t)), "lpa_set_tune")
 
     def autotune(self, cache_path=None, repeats=2) -> Tune:

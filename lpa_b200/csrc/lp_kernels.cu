@@ -1049,15 +1049,19 @@ __global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
 // segment counts and a 5-step search; the lanes of one position reserve their
 // output range with one atomicAdd on the position's cursor, since the labels
 // of a position may sit in any order.  No block barriers: warps run alone.
-// kL2Gather: residual labels are read through L2 only (ld.global.cg), leaving
-// L1 to the bitstream; without it they go through L1, which pays when a few
-// hot labels take many of the reads (lpa_tune.l2_gathers).
-template <bool kL2Gather>
+// kGather (lpa_tune.gather_cache) picks the cache path of the residual label
+// reads: 1 all through L2 only (ld.global.cg), leaving L1 to the bitstream;
+// 2 all through L1, which pays when a few hot labels take many of the reads;
+// 0 the labels of the lowest n/64 ids through L1 and the rest through L2
+// only, which on R-MAT and the copy model comes within 0.5 % of the better
+// of the two.
+template <int kGather>
 __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   __shared__ uint32_t stage[kWarps * kDecodeWindow];
   __shared__ uint8_t owner[kWarps * kDecodeWindow];
   const DevGraph &g = a.g;
   const Ctx c = resolve(a);
+  const uint32_t hot = uint32_t(g.n >> 6);  // kGather 0: ids below read through L1
   busy_mark(a, 0, false);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
@@ -1165,7 +1169,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           const uint32_t f = f0 + 32u * u + lane;
-          lv[u] = f < w1 ? (kL2Gather ? __ldcg(c.lab_in + wst[f - w0]) : ld_label(c, wst[f - w0])) : 0u;
+          const uint32_t id = f < w1 ? wst[f - w0] : 0u;
+          lv[u] = f >= w1 ? 0u
+                  : (kGather == 2 || (kGather == 0 && id < hot)) ? __ldg(c.lab_in + id)
+                                                                  : __ldcg(c.lab_in + id);
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {
@@ -1244,8 +1251,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   busy_mark(a, 0, true);
 }
 
-template __global__ void k_decode_two_pass<false>(IterArgs a);
-template __global__ void k_decode_two_pass<true>(IterArgs a);
+template __global__ void k_decode_two_pass<0>(IterArgs a);
+template __global__ void k_decode_two_pass<1>(IterArgs a);
+template __global__ void k_decode_two_pass<2>(IterArgs a);
 
 namespace {
 

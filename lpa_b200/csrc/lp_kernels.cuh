@@ -195,8 +195,8 @@ __global__ void k_batch(BatchArgs b);
 __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs);
 
 __global__ void k_iterate(IterArgs a);
-// kL2Gather: residual label reads bypass L1 (lpa_tune.l2_gathers)
-template <bool kL2Gather>
+// kGather: the cache path of the residual label reads (lpa_tune.gather_cache)
+template <int kGather>
 __global__ void k_decode_two_pass(IterArgs a);
 // V2 for tiny vertices: a lane per vertex.
 __global__ void k_packed(IterArgs a);

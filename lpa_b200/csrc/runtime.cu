@@ -532,8 +532,9 @@ static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32
   };
   mark(-1);
   if (h->n_groups) {
-    if (h->tune.l2_gathers) k_decode_two_pass<true><<<h->grid_decode, kThreads, 0, h->stream>>>(a);
-    else k_decode_two_pass<false><<<h->grid_decode, kThreads, 0, h->stream>>>(a);
+    if (h->tune.gather_cache == 1) k_decode_two_pass<1><<<h->grid_decode, kThreads, 0, h->stream>>>(a);
+    else if (h->tune.gather_cache == 2) k_decode_two_pass<2><<<h->grid_decode, kThreads, 0, h->stream>>>(a);
+    else k_decode_two_pass<0><<<h->grid_decode, kThreads, 0, h->stream>>>(a);
     h->launches++;
     mark(0);
   }
@@ -672,11 +673,12 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     occ_count = std::min(occ_count, occ_bulk);  // one grid for both forms
     h->grid_count = h->num_sms * std::max(1, occ_count);
     int occ_decode = 1;
-    int occ_l2 = 1;
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_decode, k_decode_two_pass<false>, kThreads, 0),
+    int occ_g1 = 1, occ_g2 = 1;
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_decode, k_decode_two_pass<0>, kThreads, 0),
           "occupancy");
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l2, k_decode_two_pass<true>, kThreads, 0), "occupancy");
-    occ_decode = std::min(occ_decode, occ_l2);  // one grid for both forms
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g1, k_decode_two_pass<1>, kThreads, 0), "occupancy");
+    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g2, k_decode_two_pass<2>, kThreads, 0), "occupancy");
+    occ_decode = std::min(occ_decode, std::min(occ_g1, occ_g2));  // one grid for every form
     // 960 is divisible by every resident warp count these kernels reach (16..64 in steps of 8)
     const auto weight = [](int blocks) { return uint32_t(std::max(1, 960 / (std::max(1, blocks) * kWarps))); };
     h->cw_iterate = weight(h->occ);
@@ -973,7 +975,7 @@ lpa_status lpa_set_dispatch(lpa_handle *h, int dispatch, int force_variant) {
 static bool tune_valid(const lpa_tune &t) {
   return t.group_positions >= 1 && t.group_positions <= 32 && t.warp_positions >= 1 && t.warp_positions <= 32 &&
          t.warp_max_degree >= 32 && t.warp_max_degree <= kCountWarpMax && t.warp_claim >= 1 && t.warp_claim <= 8 &&
-         t.bulk_stage <= 1 && t.l2_gathers <= 1;
+         t.bulk_stage <= 1 && t.gather_cache <= 2;
 }
 
 // One iteration from the current labels, repeated; the labels are left as
@@ -1020,7 +1022,7 @@ static std::string tune_key(const lpa_handle *h) {
   uint64_t arcs = 0;
   for (const auto &sg : h->segs) arcs += sg.arcs;
   char buf[512];
-  std::snprintf(buf, sizeof(buf), "v3|%s|sm%d|n%llu|nc%llu|arcs%llu|cms%u|plan%016llx", gpu.c_str(), pr.multiProcessorCount,
+  std::snprintf(buf, sizeof(buf), "v4|%s|sm%d|n%llu|nc%llu|arcs%llu|cms%u|plan%016llx", gpu.c_str(), pr.multiProcessorCount,
                 (unsigned long long)h->n, (unsigned long long)h->n_c, (unsigned long long)arcs,
                 h->opts.cms_threshold, (unsigned long long)fnv);
   return buf;
@@ -1059,7 +1061,7 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
         std::string k;
         lpa_tune t{};
         if (ls >> k >> t.group_positions >> t.warp_positions >> t.warp_max_degree >> t.warp_claim >> t.bulk_stage >>
-                t.l2_gathers &&
+                t.gather_cache &&
             k == key && tune_valid(t)) {
           h->tune = t;
           found = true;
@@ -1074,11 +1076,11 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
       double best_ms = tune_trial(h, repeats);
       if (best_ms < 0) throw Fail{LPA_ERR_CUDA, "autotune: " + h->last_error};
       static const uint32_t groups[] = {8, 16, 24, 32}, warps[] = {1, 2, 4, 8, 16},
-                            degs[] = {63, 127, 255, kCountWarpMax}, claims[] = {1, 2, 4, 8}, flags[] = {0, 1};
+                            degs[] = {63, 127, 255, kCountWarpMax}, claims[] = {1, 2, 4, 8}, flags[] = {0, 1, 2};
       for (int sweep = 0; sweep < 2; sweep++) {
         for (int knob = 0; knob < 6; knob++) {
           const uint32_t *vals = knob == 0 ? groups : knob == 1 ? warps : knob == 2 ? degs : knob == 3 ? claims : flags;
-          const int nv = knob == 1 ? 5 : knob >= 4 ? 2 : 4;
+          const int nv = knob == 1 ? 5 : knob == 4 ? 2 : knob == 5 ? 3 : 4;
           for (int i = 0; i < nv; i++) {
             lpa_tune cand = best;
             uint32_t &slot = knob == 0 ? cand.group_positions
@@ -1086,7 +1088,7 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
                              : knob == 2 ? cand.warp_max_degree
                              : knob == 3 ? cand.warp_claim
                              : knob == 4 ? cand.bulk_stage
-                                         : cand.l2_gathers;
+                                         : cand.gather_cache;
             if (slot == vals[i]) continue;
             slot = vals[i];
             h->tune = cand;
@@ -1105,7 +1107,7 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
       if (cache_path) {
         std::ofstream o(cache_path, std::ios::app);
         o << key << ' ' << best.group_positions << ' ' << best.warp_positions << ' ' << best.warp_max_degree << ' '
-          << best.warp_claim << ' ' << best.bulk_stage << ' ' << best.l2_gathers << ' ' << best_ms << '\n';
+          << best.warp_claim << ' ' << best.bulk_stage << ' ' << best.gather_cache << ' ' << best_ms << '\n';
       }
     }
     if (out) *out = h->tune;

@@ -21,11 +21,11 @@ def _two_pass(p):
     p.set_plan(plan)
 
 
-@pytest.mark.parametrize("knobs", [(1, 1, 32, 1, 0, 0), (7, 3, 100, 8, 1, 1), (32, 32, 511, 5, 0, 1),
+@pytest.mark.parametrize("knobs", [(1, 1, 32, 1, 0, 0), (7, 3, 100, 8, 1, 1), (32, 32, 511, 5, 0, 2),
                                    (32, 4, 511, 2, 1, 0)])
 def test_knobs_keep_labels_exact(knobs):
     """bulk_stage = 1 stages the several-vertices items by bulk copies;
-    l2_gathers = 1 reads the pre-pass's labels through L2 only."""
+    gather_cache picks the pre-pass's label read path (hot ids / L2 / L1)."""
     g, ref = _load("rmat_t16")
     hist, changed = oracle.lp_run(ref["row"], ref["clm"], 4, 64)
     with L.Propagator(g, cms_threshold=64) as p:
@@ -42,7 +42,7 @@ def test_out_of_range_knobs_are_refused():
     with L.Propagator(g) as p:
         before = p.get_tune().as_tuple()
         for bad in [(0, 4, 511, 2), (33, 4, 511, 2), (32, 4, 31, 2), (32, 4, 512, 2), (32, 4, 511, 9),
-                    (32, 4, 511, 2, 2), (32, 4, 511, 2, 0, 2)]:
+                    (32, 4, 511, 2, 2), (32, 4, 511, 2, 0, 3)]:
             with pytest.raises(L.LpaError) as e:
                 p.set_tune(*bad)
             assert e.value.status == L.Status.INVALID_ARG
