@@ -322,7 +322,8 @@ __device__ __forceinline__ int64_t walk_vertex_buf(const uint32_t *__restrict__ 
     last = r.pos();
   }
   if (interval_items) *interval_items = cnt_all;
-  r.seek(words, last);
+  // the reader already stands at `last`: the residual section follows the last
+  // interval segment's final item (or the empty interval section)
   nseg = r.segcnt(bad);
   const uint64_t rbase = r.pos();
   last = r.pos();
