@@ -9,7 +9,7 @@
 //
 // Schedule of a handle in LPA_DISPATCH_LEARNED:
 //   1. one iteration on the fixed degree-bucket plan: its device time is the
-//      reference (the judge);
+//      yardstick every learned plan must beat;
 //   2. kExplore iterations on round-robin plans (segment s runs its
 //      ((s + k) mod capable)-th capable variant) -- every step trains the MLP;
 //   3. the MLP's plan runs, then (when it differs) the same plan with every
@@ -374,7 +374,7 @@ void lpa_learner_after_iteration(lpa_handle *h) {
   h->collect_cycles = false;
   Learner *L = h->learner;
   if (!L || h->opts.dispatch != LPA_DISPATCH_LEARNED) return;
-  // The judge's clock: the time the iteration's kernels were busy on the GPU
+  // The yardstick's clock: the time the iteration's kernels were busy on the GPU
   // (the sum of their spans on the GPU clock).  Unlike the events around the
   // iteration, it leaves out host-side gaps between launches, which a tool
   // such as a profiler can stretch by orders of magnitude.
