@@ -1151,18 +1151,29 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
     uint32_t done = 0, v = 0;
     for (uint32_t w0 = 0; w0 < rtot; w0 += kDecodeWindow) {
       const uint32_t w1 = min(w0 + kDecodeWindow, rtot);
-      while (done < ritems && rexcl + done < w1) {
-        const uint32_t x = r.zeta3(bad);
-        v = (done == 0) ? zigzag_first(node, x) : v + x + 1u;
-        uint32_t id = v;
-        if (bad || uint64_t(v) >= g.n) {  // the segment's end is checked once, below
-          bad = true;
-          id = node;  // in range; the error word reports the stream
-        }
-        wst[rexcl + done - w0] = id;
-        wown[rexcl + done - w0] = uint8_t(lane);
-        done++;
+      // this lane's items up to `lim` fall in this window, item i at window
+      // index rexcl + i - w0 (>= 0 for every item not yet written)
+      const uint32_t lim = rexcl + done < w1 ? min(ritems, w1 - rexcl) : done;
+      uint32_t *dst = wst + (int32_t(rexcl) - int32_t(w0));
+      uint8_t *own = wown + (int32_t(rexcl) - int32_t(w0));
+      bool oob = false;
+      if (done == 0 && lim > 0) {
+        v = zigzag_first(node, r.zeta3(bad));
+        oob |= uint64_t(v) >= g.n;
+        dst[0] = oob ? node : v;
+        own[0] = uint8_t(lane);
+        done = 1;
       }
+      for (; done < lim; done++) {
+        v += r.zeta3(bad) + 1u;
+        // an id out of range reads the vertex's own label; the error word
+        // reports the stream (its end is checked once, below)
+        const bool out = uint64_t(v) >= g.n;
+        oob |= out;
+        dst[done] = out ? node : v;
+        own[done] = uint8_t(lane);
+      }
+      bad |= oob;
       __syncwarp();
       for (uint32_t f0 = w0; f0 < w1; f0 += 256) {
         uint32_t lv[8];
