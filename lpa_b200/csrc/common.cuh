@@ -219,9 +219,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
 
 struct BitReader {
   const uint32_t *__restrict__ w;
-  uint64_t buf;    // upcoming bits, MSB-aligned
-  uint64_t wnext;  // next word to load into buf
-  uint32_t nb;     // valid bits in buf
+  uint32_t hi, lo;  // upcoming bits, MSB-aligned: hi the next 32, lo the 32 after (zero past the valid bits)
+  uint64_t wnext;   // next word to load
+  uint32_t nb;      // valid bits in hi:lo
 
   // absolute position of the next unread bit (kept implicit: every code
   // would otherwise pay a 64-bit add)
@@ -230,27 +230,31 @@ struct BitReader {
     w = words;
     const uint64_t i = p >> 5;
     const uint32_t s = uint32_t(p) & 31u;
-    const uint64_t a = __ldg(w + i), b = __ldg(w + i + 1);
-    buf = ((a << 32) | b) << s;
+    const uint32_t a = __ldg(w + i), b = __ldg(w + i + 1);
+    hi = __funnelshift_l(b, a, s);
+    lo = b << s;
     nb = 64 - s;
     wnext = i + 2;
   }
+  // Tops the buffer up to at least 33 valid bits (from at least 1).
   __device__ __forceinline__ void fill() {
-    if (nb <= 32) {
-      buf |= uint64_t(__ldg(w + wnext)) << (32 - nb);
+    if (nb <= 32) {  // every valid bit is in hi and lo is zero
+      const uint32_t x = __ldg(w + wnext);
+      hi |= __funnelshift_rc(x, 0u, nb);  // x >> nb, 0 when nb == 32
+      lo = x << (32 - nb);
       wnext++;
       nb += 32;
     }
   }
-  __device__ __forceinline__ void skip(uint32_t k) {  // k < 64, k <= nb
-    buf <<= k;
+  __device__ __forceinline__ void skip(uint32_t k) {  // k <= 32, k <= nb
+    hi = __funnelshift_lc(lo, hi, k);
+    lo = __funnelshift_lc(0u, lo, k);  // lo << k, 0 when k == 32
     nb -= k;
   }
-  // After fill() the top 32 bits of buf are valid (nb >= 33); a fast-path
-  // code lies within them, so its fields come from 32-bit shifts.
+  // After fill() hi is all valid bits (nb >= 33); a fast-path code lies
+  // within it, so its fields come from 32-bit shifts.
   __device__ __forceinline__ uint32_t gamma(bool &bad) {
     fill();
-    const uint32_t hi = uint32_t(buf >> 32);
     const uint32_t z = __clz(hi);
     if (z < 16) {  // 2z+1 <= 31 bits
       const uint32_t len = 2 * z + 1;
@@ -265,7 +269,6 @@ struct BitReader {
   }
   __device__ __forceinline__ uint32_t zeta3(bool &bad) {
     fill();
-    const uint32_t hi = uint32_t(buf >> 32);
     const uint32_t h = __clz(hi);
     if (h < 8) {  // 4(h+1) <= 32 bits
       const uint32_t v = (hi << (h + 1)) >> (32 - 3 * (h + 1));
@@ -279,8 +282,8 @@ struct BitReader {
   }
   __device__ __forceinline__ uint32_t segcnt(bool &bad) {
     fill();
-    if (buf >> 63) {
-      if ((buf >> 62) & 1ull) {
+    if (hi >> 31) {
+      if ((hi >> 30) & 1u) {
         skip(2);
         return 0;
       }
