@@ -1146,6 +1146,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
     const uint32_t rincl = warp_incl_scan(ritems, lane);
     const uint32_t rexcl = rincl - ritems;
     const uint32_t rtot = __shfl_sync(kFull, rincl, 31);
+    // window item f of lane l goes to scratch[gb + drel_l + f] (32-bit
+    // arithmetic) when the group's residual items lie within 2^32 of lane 0's
+    // first, which holds the lowest scratch index of the group
+    const uint64_t gb = (uint64_t(__shfl_sync(kFull, uint32_t(obase >> 32), 0)) << 32) |
+                        __shfl_sync(kFull, uint32_t(obase), 0);
+    const bool rel32 = __all_sync(kFull, ritems == 0u || ((obase + ritems - gb) >> 32) == 0ull);
+    const uint32_t drel = uint32_t(obase - gb) - rexcl;
     uint32_t *wst = stage + warp * kDecodeWindow;
     uint8_t *wown = owner + warp * kDecodeWindow;
     uint32_t done = 0, v = 0;
@@ -1185,14 +1192,24 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
                   : (kGather == 2 || (kGather == 0 && id < hot)) ? __ldg(c.lab_in + id)
                                                                   : __ldcg(c.lab_in + id);
         }
+        if (rel32) {
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const uint32_t f = f0 + 32u * u + lane;
-          const uint32_t ol = f < w1 ? wown[f - w0] : 0u;
-          const uint64_t ob = (uint64_t(__shfl_sync(kFull, uint32_t(obase >> 32), ol)) << 32) |
-                              __shfl_sync(kFull, uint32_t(obase), ol);
-          const uint32_t ox = __shfl_sync(kFull, rexcl, ol);
-          if (f < w1) a.scratch[ob + (f - ox)] = lv[u];
+          for (int u = 0; u < 8; u++) {
+            const uint32_t f = f0 + 32u * u + lane;
+            const uint32_t ol = f < w1 ? wown[f - w0] : 0u;
+            const uint32_t rel = __shfl_sync(kFull, drel, ol) + f;
+            if (f < w1) a.scratch[gb + rel] = lv[u];
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            const uint32_t f = f0 + 32u * u + lane;
+            const uint32_t ol = f < w1 ? wown[f - w0] : 0u;
+            const uint64_t ob = (uint64_t(__shfl_sync(kFull, uint32_t(obase >> 32), ol)) << 32) |
+                                __shfl_sync(kFull, uint32_t(obase), ol);
+            const uint32_t ox = __shfl_sync(kFull, rexcl, ol);
+            if (f < w1) a.scratch[ob + (f - ox)] = lv[u];
+          }
         }
       }
       __syncwarp();
