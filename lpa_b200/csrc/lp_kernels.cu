@@ -1673,6 +1673,36 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
 template __global__ void k_count_two_pass<false>(IterArgs a);
 template __global__ void k_count_two_pass<true>(IterArgs a);
 
+void launch_decode_two_pass(uint32_t gather_cache, int grid, cudaStream_t s, const IterArgs &a) {
+  if (gather_cache == 1) k_decode_two_pass<1><<<grid, kThreads, 0, s>>>(a);
+  else if (gather_cache == 2) k_decode_two_pass<2><<<grid, kThreads, 0, s>>>(a);
+  else k_decode_two_pass<0><<<grid, kThreads, 0, s>>>(a);
+}
+
+void launch_count_two_pass(bool bulk, int grid, cudaStream_t s, const IterArgs &a) {
+  if (bulk) k_count_two_pass<true><<<grid, kThreads, kCountSmemBytes, s>>>(a);
+  else k_count_two_pass<false><<<grid, kThreads, kCountSmemBytes, s>>>(a);
+}
+
+cudaError_t occupancy_decode_two_pass(int *blocks) {
+  int b0 = 1, b1 = 1, b2 = 1;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_decode_two_pass<0>, kThreads, 0);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_decode_two_pass<1>, kThreads, 0);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_decode_two_pass<2>, kThreads, 0);
+  *blocks = b0 < b1 ? (b0 < b2 ? b0 : b2) : (b1 < b2 ? b1 : b2);
+  return e;
+}
+
+cudaError_t occupancy_count_two_pass(int *blocks) {
+  int b0 = 1, b1 = 1;
+  cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_count_two_pass<false>, kThreads, kCountSmemBytes);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_count_two_pass<true>, kThreads, kCountSmemBytes);
+  *blocks = b0 < b1 ? b0 : b1;
+  return e;
+}
+
 __global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err) {
   for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < g.n_c;
        p += uint64_t(gridDim.x) * blockDim.x) {

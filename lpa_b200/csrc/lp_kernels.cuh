@@ -205,6 +205,16 @@ __global__ void k_packed(IterArgs a);
 template <bool kBulk>
 __global__ void k_count_two_pass(IterArgs a);
 
+// The template forms of the two-pass kernels are launched and sized only in
+// the file that defines them (lp_kernels.cu):
+// k_decode_two_pass<gather_cache> on `grid` blocks of kThreads;
+void launch_decode_two_pass(uint32_t gather_cache, int grid, cudaStream_t s, const IterArgs &a);
+// k_count_two_pass<bulk> on `grid` blocks of kThreads with kCountSmemBytes;
+void launch_count_two_pass(bool bulk, int grid, cudaStream_t s, const IterArgs &a);
+// the fewest resident blocks per SM over each kernel's forms.
+cudaError_t occupancy_decode_two_pass(int *blocks);
+cudaError_t occupancy_count_two_pass(int *blocks);
+
 struct DecodeArgs {
   DevGraph g;
   const uint32_t *pos_list;  // positions to decode (nullptr: all of [0, n_pos))

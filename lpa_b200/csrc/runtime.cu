@@ -532,15 +532,12 @@ static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32
   };
   mark(-1);
   if (h->n_groups) {
-    if (h->tune.gather_cache == 1) k_decode_two_pass<1><<<h->grid_decode, kThreads, 0, h->stream>>>(a);
-    else if (h->tune.gather_cache == 2) k_decode_two_pass<2><<<h->grid_decode, kThreads, 0, h->stream>>>(a);
-    else k_decode_two_pass<0><<<h->grid_decode, kThreads, 0, h->stream>>>(a);
+    launch_decode_two_pass(h->tune.gather_cache, h->grid_decode, h->stream, a);
     h->launches++;
     mark(0);
   }
   if (h->n_cblock + h->n_cwarp) {
-    if (h->tune.bulk_stage) k_count_two_pass<true><<<h->grid_count, kThreads, kCountSmemBytes, h->stream>>>(a);
-    else k_count_two_pass<false><<<h->grid_count, kThreads, kCountSmemBytes, h->stream>>>(a);
+    launch_count_two_pass(h->tune.bulk_stage != 0, h->grid_count, h->stream, a);
     h->launches++;
     mark(1);
   }
@@ -663,22 +660,11 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ, k_iterate, kThreads, kSmemBytes), "occupancy");
     h->occ = std::max(1, h->occ);
     h->grid = h->num_sms * h->occ;
-    int occ_count = 1, occ_bulk = 1;
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_count, k_count_two_pass<false>, kThreads,
-                                                           kCountSmemBytes),
-          "occupancy");
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_bulk, k_count_two_pass<true>, kThreads,
-                                                           kCountSmemBytes),
-          "occupancy");
-    occ_count = std::min(occ_count, occ_bulk);  // one grid for both forms
+    int occ_count = 1;  // one grid for both forms
+    check(h, occupancy_count_two_pass(&occ_count), "occupancy");
     h->grid_count = h->num_sms * std::max(1, occ_count);
-    int occ_decode = 1;
-    int occ_g1 = 1, occ_g2 = 1;
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_decode, k_decode_two_pass<0>, kThreads, 0),
-          "occupancy");
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g1, k_decode_two_pass<1>, kThreads, 0), "occupancy");
-    check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g2, k_decode_two_pass<2>, kThreads, 0), "occupancy");
-    occ_decode = std::min(occ_decode, std::min(occ_g1, occ_g2));  // one grid for every form
+    int occ_decode = 1;  // one grid for every form
+    check(h, occupancy_decode_two_pass(&occ_decode), "occupancy");
     // 960 is divisible by every resident warp count these kernels reach (16..64 in steps of 8)
     const auto weight = [](int blocks) { return uint32_t(std::max(1, 960 / (std::max(1, blocks) * kWarps))); };
     h->cw_iterate = weight(h->occ);
