@@ -31,6 +31,17 @@ def test_symbol_exported(name):
     assert hasattr(lib, name), name
 
 
+def test_library_binds_every_symbol_at_load():
+    """Immediate binding in a fresh process: no symbol is left undefined for a
+    later call to trip over."""
+    import subprocess
+    import sys
+
+    code = f"import ctypes, os; ctypes.CDLL({str(L.LIB_PATH)!r}, mode=os.RTLD_NOW)"
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+
+
 def test_status_strings():
     lib = L.lib()
     for s in L.Status:
