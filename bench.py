@@ -323,8 +323,90 @@ def cpu_baseline(arr: dict, w: dict, budget_s: float = 12.0) -> dict:
         times.append(time.perf_counter() - t0)
     row_arcs = oracle.range_arcs(arr, 0, p_end)
     t = statistics.median(times)
-    return {"value": row_arcs / t, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": row_arcs / t, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
             "sample": f"positions [0,{p_end}) of {n} ({row_arcs} arcs), median of 3 iterations after 1 warm-up"}
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_compressor_sample() -> dict | None:
+    """The reference's own CPU compressor (CgrCompressor::compresswithcost,
+    built from the reference sources into oracle/_ref/cgr_ref) on a bounded
+    sample: R-MAT scale 19, edge factor 16, threshold 32, one thread (the
+    reference compressor is single-threaded).  None when it was not built."""
+    import re
+
+    import lpa_b200 as L
+
+    exe = ROOT / "oracle" / "_ref" / "cgr_ref"
+    if not exe.exists():
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        g = L.HostGraph.rmat(19, 16.0, seed=1)
+        arcs = int(len(g.csr()[1]))
+        path = str(Path(td) / "rmat19.txt")
+        g.write_edge_list(path, False)
+        t0 = time.perf_counter()
+        r = subprocess.run([str(exe), path, "1", "32"], capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        m = re.search(r"without I/O:\s*([0-9.eE+-]+)", r.stdout)
+        ours0 = time.perf_counter()
+        g.compress(32, 128, threads=1)
+        ours = time.perf_counter() - ours0
+    if r.returncode != 0 or not m:
+        return {"error": f"cgr_ref exited {r.returncode}"}
+    sec = float(m.group(1))
+    return {"sample": "R-MAT scale 19, edge factor 16, threshold 32 (edge list written as the reference's text)",
+            "arcs": arcs, "compresswithcost_s": sec, "with_io_s": wall, "arcs_per_s": arcs / sec,
+            "this_library_1_thread_s": ours}
+
+
+def cpu_baseline_and_verify(p, arr: dict, w: dict) -> dict:
+    """The oracle's OpenMP CPU path (decode + synchronous LP, same rule) on the
+    whole workload, iterations 1..iters from the initial labels: timed, it is
+    the CPU baseline; beside it the GPU runs the same iterations on the plan
+    and knobs of the timed region, and its labels and changed count are
+    compared with the oracle's after every iteration (outside any timed
+    region)."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    n = arr["n"]
+    iters = w["iters"]
+    lab = np.arange(n, dtype=np.uint32)
+    p.init_labels()
+    times = []
+    mismatches = changed_mismatches = 0
+    first_bad = None
+    for it in range(iters):
+        gch = p.iterate()
+        glab = p.labels()
+        t0 = time.perf_counter()
+        nxt, och = oracle.lp_iterate_cgr(arr, lab, w["cms"], 1, threads)
+        times.append(time.perf_counter() - t0)
+        bad = int(np.count_nonzero(glab != nxt))
+        mismatches += bad
+        changed_mismatches += int(gch != och)
+        if (bad or gch != och) and first_bad is None:
+            first_bad = {"iteration": it + 1, "labels": bad, "changed": [int(gch), int(och)]}
+        lab = nxt
+    arcs = oracle.range_arcs(arr, 0, n)
+    t = sum(times)
+    cb = {"value": arcs * iters / t, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
+          "sample": f"the whole workload ({arcs} arcs), iterations 1..{iters} from the initial labels, "
+                    f"{t:.1f} s; the oracle's OpenMP decode + LP loop",
+          "reference_compressor": reference_compressor_sample()}
+    verify = {"iterations": iters, "mismatches": mismatches, "changed_mismatches": changed_mismatches,
+              "first_mismatch": first_bad, "oracle": "oracle.lp_iterate_cgr (CPU restatement of the update rule)"}
+    return cb, verify
 
 
 def run_reference(args, w, rank, world):
@@ -492,9 +574,9 @@ def main():
     e2e_s = max_over_ranks(time.perf_counter() - e0, world, device)
     e2e_value = arcs * args.e2e_steps * world / e2e_s
 
-    cb = None
+    cb = verify = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(arr, w)
+        cb, verify = cpu_baseline_and_verify(p, arr, w)
 
     if rank == 0:
         line = {
@@ -521,6 +603,7 @@ def main():
                          "learned_over_fixed": (fixed_ms / total_ms) if args.dispatch == "learned" else None,
                          "learner": learned_info},
             "cpu_baseline": cb,
+            "verify": verify,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * arr["n"],
                     "d2h_bytes_per_step": 4 * arr["n"] + 8},
             "gpu_launches": int(st1.launches - st0.launches),

@@ -85,6 +85,11 @@ typedef struct lpa_opts {
   int record_timings;      /* 1: per-launch events; 2: also per-segment device cycles */
   int verbose;             /* per-iteration log lines on stdout */
   int batch_mode;          /* lpa_batch_mode, for lpa_batch_create */
+  /* LPA_BATCH_QUEUE: how many times (about 200 ns each) a block of the
+   * persistent kernel looks at an empty queue slot, while graphs are still
+   * running, before it gives up and the run returns LPA_ERR_TIMEOUT.
+   * 0: the default, 2^25 (about 7 s). */
+  uint64_t queue_wait_limit;
 } lpa_opts;
 
 typedef enum lpa_batch_mode {
@@ -229,8 +234,10 @@ lpa_status lpa_get_segment_cycles(struct lpa_handle *h, uint64_t *cycles, size_t
  * reference.
  *   g          : every pointer in it is DEVICE memory owned by the caller; the
  *                stream words need at least 4 zero words after the last bit.
- *   labels_in / labels_out : device, n entries each, distinct buffers; every
- *                vertex's output is written.
+ *                g->vertices must be a permutation of 0..n-1 (as every
+ *                compressor output is).
+ *   labels_in / labels_out : device, n entries each, distinct buffers; with
+ *                vertices a permutation, every vertex's output is written.
  *   stream     : cudaStream_t (NULL: the legacy default stream).
  *   changed_out: host, may be NULL.
  * Working memory is one static 16 MiB device array inside the library, held
@@ -238,8 +245,13 @@ lpa_status lpa_get_segment_cycles(struct lpa_handle *h, uint64_t *cycles, size_t
  * decoded ids of the compressed positions must fit in it, and every degree
  * must be <= 1023 and below cms_threshold (when non-zero); otherwise the call
  * returns LPA_ERR_CAPACITY without launching the decode.  The first call on a
- * device looks up the array's address; make it before any stream capture.
- * Calls whose work overlaps on the GPU race on the shared array. */
+ * device looks up the array's address, which also makes the device load the
+ * library's kernels and claim the array (lazy module loading): make it before
+ * the caller spends its memory budget and before any stream capture.  It
+ * returns LPA_ERR_OOM when the device cannot hold the array.  The address is
+ * kept for the process's life: resetting the device (cudaDeviceReset) after
+ * it is not supported.  One array serves every call on a device: calls whose
+ * work overlaps on the GPU (other streams, other host threads) race on it. */
 lpa_status lpa_iterate_noalloc(const lpa_graph_desc *g, const uint32_t *labels_in, uint32_t *labels_out,
                                uint32_t cms_threshold, void *stream, uint64_t *changed_out);
 

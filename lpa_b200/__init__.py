@@ -105,6 +105,7 @@ class Opts(C.Structure):
         ("record_timings", C.c_int),
         ("verbose", C.c_int),
         ("batch_mode", C.c_int),
+        ("queue_wait_limit", C.c_uint64),
     ]
 
 

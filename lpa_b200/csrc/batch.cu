@@ -526,7 +526,8 @@ lpa_status lpa_batch_run(lpa_batch *b, int max_iter, int early_exit, uint32_t *i
         for (int r = 0; r < kCmsDepth; r++) a.seeds[r] = b->seeds[r];
         a.gtab = b->d_gtab;
         a.gtab_slots = b->gtab_slots;
-        a.spin_limit = 1ull << 25;  // ~7 s of 200 ns sleeps with nothing to do
+        // ~7 s of 200 ns sleeps with nothing to do, unless the caller bounds it
+        a.spin_limit = b->opts.queue_wait_limit ? b->opts.queue_wait_limit : (1ull << 25);
         k_batch<<<b->num_sms * b->occ, kThreads, kSmemBytes, b->stream>>>(a);
         bcheck(cudaGetLastError());
       }

@@ -12,8 +12,12 @@
 // there.
 //
 // Set-up: the first call on a device looks up the array's device address with
-// cudaGetSymbolAddress, with that device current, and keeps it. Make that
-// first call before any stream capture.
+// cudaGetSymbolAddress, with that device current, and keeps it. The library
+// loads its device code lazily, so that first call is also when the device
+// claims the 16 MiB array and loads these kernels: make it before the caller
+// spends its memory budget, and before any stream capture. The address is
+// kept for the life of the process; a reset of the device's primary context
+// (cudaDeviceReset) is not supported afterwards.
 //
 // Sharing: every call uses the same array, which keeps the last call's
 // contents. The counters are cleared at the start of every call. Calls whose
@@ -54,7 +58,8 @@ lpa_status scratch_for_current_device(unsigned char **out) {
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
       cudaGetLastError();
-      return LPA_ERR_CUDA;
+      // loading the module that holds the array is what allocates it
+      return e == cudaErrorMemoryAllocation ? LPA_ERR_OOM : LPA_ERR_CUDA;
     }
     g_scratch_ptr[dev] = static_cast<unsigned char *>(p);
   }

@@ -6,7 +6,8 @@ namespace lpa_dev {
 
 // ---- one two-pass iteration over caller-owned device buffers ------------
 // The decoded CSR, the per-position degrees and offsets and the counters live
-// in a caller-supplied scratch region (see noalloc.cu).
+// in the library's static device array (g_noalloc_scratch in noalloc.cu), not
+// in caller memory.
 struct NoAllocArgs {
   DevGraph g;                   // g.deg points into the scratch region
   uint32_t *deg;                // n degrees by position

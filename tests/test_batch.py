@@ -122,3 +122,20 @@ def test_lockstep_rejects_foreign_ids():
     for mode in MODES:
         with pytest.raises(L.LpaError):
             L.Batch([bad, a], batch_mode=mode)
+
+
+def test_queue_wait_that_runs_out_returns_timeout():
+    """The persistent queue's wait for an item is bounded.  With a bound of one
+    try, the many blocks that find no item while the graphs still run give up
+    at once: the kernel sets the timeout error and returns (it does not trap),
+    the run reports LPA_ERR_TIMEOUT, and the context stays usable."""
+    graphs = _graphs()[:4]
+    with L.Batch(graphs, batch_mode=L.BatchMode.QUEUE, queue_wait_limit=1) as b:
+        with pytest.raises(L.LpaError) as e:
+            b.run(30, early_exit=True)
+        assert e.value.status == L.Status.TIMEOUT
+    # the device still works: the same batch with the default bound
+    with L.Batch(graphs, batch_mode=L.BatchMode.QUEUE) as b:
+        iters = b.run(30, early_exit=True)
+        for i, g in enumerate(graphs):
+            assert np.array_equal(b.labels(i), _alone(g, 30, 0, True)[-1])

@@ -106,3 +106,75 @@ def test_noalloc_rejects_beyond_its_limits():
     st, _ = _call(desc, a, b)
     assert st == L.Status.CAPACITY
     del keep
+
+
+def _dense_random_graph(n, per_vertex, seed):
+    """Undirected random graph: every vertex draws per_vertex partners."""
+    rng = np.random.default_rng(seed)
+    src = np.repeat(np.arange(n, dtype=np.int64), per_vertex)
+    dst = rng.integers(0, n, size=src.size)
+    keep = src != dst
+    a = np.concatenate([src[keep], dst[keep]])
+    b = np.concatenate([dst[keep], src[keep]])
+    key = np.unique(a * n + b)
+    a, b = key // n, key % n
+    row = np.zeros(n + 1, np.uint64)
+    np.add.at(row, a + 1, 1)
+    row = np.cumsum(row).astype(np.uint64)
+    return row, b.astype(np.uint32)
+
+
+def test_noalloc_refuses_ids_beyond_its_array():
+    """4.9M decoded ids (degrees <= 1023) exceed the 16 MiB array: CAPACITY."""
+    torch = pytest.importorskip("torch")
+    n = 8192
+    row, clm = _dense_random_graph(n, 300, seed=3)
+    assert int(np.diff(row.astype(np.int64)).max()) <= 1023 and len(clm) > (16 << 20) // 4
+    g = L.HostGraph.from_csr(row, clm).compress(0, 128)
+    desc, keep = _device_desc(torch, g.arrays())
+    a = torch.arange(n, dtype=torch.int32, device="cuda:0")
+    b = torch.empty(n, dtype=torch.int32, device="cuda:0")
+    st, _ = _call(desc, a, b)
+    assert st == L.Status.CAPACITY
+    del keep
+
+
+def test_noalloc_refuses_a_vertex_at_the_sketch_threshold():
+    torch = pytest.importorskip("torch")
+    g = L.HostGraph.road(64, 48, seed=5).compress(0, 128)
+    row, _ = g.csr()
+    dmax = int(np.diff(row.astype(np.int64)).max())
+    desc, keep = _device_desc(torch, g.arrays())
+    n = g.arrays()["n"]
+    a = torch.arange(n, dtype=torch.int32, device="cuda:0")
+    b = torch.empty(n, dtype=torch.int32, device="cuda:0")
+    st, _ = _call(desc, a, b, cms_thr=dmax)
+    assert st == L.Status.CAPACITY
+    # one above the largest degree: every vertex is exact, so the call runs
+    st, _ = _call(desc, a, b, cms_thr=dmax + 1)
+    assert st == 0
+    del keep
+
+
+def test_noalloc_small_csr_only_matches_regular_entry_point():
+    """Every vertex below the compression threshold (no compressed position):
+    the decode steps are skipped and only the small CSR is counted."""
+    torch = pytest.importorskip("torch")
+    g = L.HostGraph.road(96, 80, seed=6).compress(32, 128)
+    arr = g.arrays()
+    assert arr["n_c"] == 0
+    n = arr["n"]
+    desc, keep = _device_desc(torch, arr)
+    a = torch.arange(n, dtype=torch.int32, device="cuda:0")
+    b = torch.full((n,), -1, dtype=torch.int32, device="cuda:0")
+    c = torch.full((n,), -1, dtype=torch.int32, device="cuda:0")
+    with L.Propagator(g) as p:
+        st, ch1 = _call(desc, a, b)
+        assert st == 0
+        assert ch1 == p.iterate()
+        assert np.array_equal(b.cpu().numpy().view(np.uint32), p.labels())
+        st, ch2 = _call(desc, b, c)
+        assert st == 0
+        assert ch2 == p.iterate()
+        assert np.array_equal(c.cpu().numpy().view(np.uint32), p.labels())
+    del keep
