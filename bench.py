@@ -409,6 +409,47 @@ def cpu_baseline_and_verify(p, arr: dict, w: dict) -> dict:
     return cb, verify
 
 
+def dispatch_report(p, fixed_plan, steps: int, timed_region) -> dict:
+    """Iterations 1..steps from the initial labels on explicit plans, each timed
+    like the main region: the cost model's own plan (before the learner's
+    trials), the merged candidate (its plan with every capable segment on the
+    two-pass kernels), and every single-variant plan (each segment on that
+    variant where it can run, else the fixed plan's choice).  The learner is
+    reset by the first explicit plan, so this runs last."""
+    import lpa_b200 as L
+
+    cap = p.capable()
+    plans = {}
+    try:
+        mlp = p.mlp_plan()
+    except L.LpaError:
+        mlp = None
+    if mlp is not None:
+        plans["mlp_plan"] = mlp
+        merged = mlp.copy()
+        two = int(L.Variant.TWO_PASS)
+        merged[(cap >> two) & 1 == 1] = two
+        plans["merged"] = merged
+    for v in L.Variant:
+        plan = fixed_plan.copy()
+        ok = (cap >> int(v)) & 1 == 1
+        plan[ok] = int(v)
+        plans[f"all_{v.name.lower()}"] = plan
+    out = {}
+    for name, plan in plans.items():
+        p.set_plan(plan)
+        p.init_labels()
+        ms, _ = timed_region(steps)
+        out[name] = ms / steps
+    static = {k: v for k, v in out.items() if k.startswith("all_")}
+    best = min(static, key=static.get)
+    rep = {"mlp_plan_ms": out.get("mlp_plan"), "merged_ms": out.get("merged"), "best_static_ms": static[best],
+           "best_static": best, "static_ms": static,
+           "mlp_plan_variant_segments": [int((plans["mlp_plan"] == v).sum()) for v in range(4)]
+           if "mlp_plan" in plans else None}
+    return rep
+
+
 def run_reference(args, w, rank, world):
     if rank != 0:
         return
@@ -442,6 +483,8 @@ def main():
     ap.add_argument("--batch-mode", default="lockstep", choices=["lockstep", "queue"],
                     help="batched workloads: the concatenated graph in lockstep, or the persistent queue")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-dispatch-report", dest="dispatch_report", action="store_false",
+                    help="skip timing the cost model's own plan and the single-variant plans after the run")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     w = WORKLOADS[args.workload]
@@ -477,6 +520,7 @@ def main():
     p = L.Propagator(L.desc_from_arrays(arr), device=local, cms_threshold=w["cms"], cms_seed=1,
                      record_timings=1, stream=stream.cuda_stream, dispatch=L.Dispatch.FIXED)
     info = p.get_info()
+    fixed_plan = p.current_plan()
     arcs = int(info.num_arcs)
     b_alg = int(info.bytes_algorithmic)
     inputs_bytes = b_alg
@@ -577,6 +621,11 @@ def main():
     cb = verify = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, verify = cpu_baseline_and_verify(p, arr, w)
+    report = None
+    if args.dispatch == "learned" and args.dispatch_report:
+        report = dispatch_report(p, fixed_plan, args.steps, timed_region)
+        report["learned_ms"] = ms_per_step
+        report["fixed_ms"] = fixed_ms / args.steps
 
     if rank == 0:
         line = {
@@ -601,7 +650,7 @@ def main():
                          "fixed_value": arcs * args.steps * world / (fixed_ms / 1e3),
                          "fixed_ms_per_step": fixed_ms / args.steps,
                          "learned_over_fixed": (fixed_ms / total_ms) if args.dispatch == "learned" else None,
-                         "learner": learned_info},
+                         "learner": learned_info, "plans": report},
             "cpu_baseline": cb,
             "verify": verify,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * arr["n"],

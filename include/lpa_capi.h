@@ -204,6 +204,9 @@ lpa_status lpa_set_tune(struct lpa_handle *h, const lpa_tune *t);
  * and a new result is appended.  The best knobs are installed and returned in
  * out (may be NULL). */
 lpa_status lpa_autotune(struct lpa_handle *h, const char *cache_path, int repeats, lpa_tune *out);
+/* Per segment, a bit mask of the variants able to run it (bit v: lpa_variant
+ * v), the plans lpa_set_plan accepts. */
+lpa_status lpa_get_capable(struct lpa_handle *h, uint8_t *mask, size_t count);
 /* Per-segment view of the plan: begin/end positions, bucket, variant. */
 lpa_status lpa_get_segments(struct lpa_handle *h, uint32_t *begin, uint32_t *end, uint8_t *bucket,
                             uint8_t *variant, size_t count);
@@ -223,6 +226,12 @@ lpa_status lpa_mlp_predict(int device, const float *params, const float *x, size
 lpa_status lpa_get_mlp(struct lpa_handle *h, float *params, size_t n);
 /* The last learned plan (variant per segment) and its predictions (4 per segment). */
 lpa_status lpa_get_learned_plan(struct lpa_handle *h, uint8_t *plan, float *pred, size_t count);
+/* The cost model's own plan: per segment, the capable variant with the least
+ * predicted cost, as the model gave it after exploring -- before the learner's
+ * trials compare it with the merged candidate (every capable segment on the
+ * two-pass kernels) and with the fixed plan.  LPA_ERR_INVALID_ARG until the
+ * learner has explored. */
+lpa_status lpa_get_mlp_plan(struct lpa_handle *h, uint8_t *plan, size_t count);
 /* Device cycles per segment of the last iteration that recorded them. */
 lpa_status lpa_get_segment_cycles(struct lpa_handle *h, uint64_t *cycles, size_t count);
 

@@ -209,6 +209,8 @@ def lib():
     _sig(L, "lpa_get_mlp", [P, fp, C.c_size_t])
     _sig(L, "lpa_get_learned_plan", [P, u8p, fp, C.c_size_t])
     _sig(L, "lpa_get_segment_cycles", [P, u64p, C.c_size_t])
+    _sig(L, "lpa_get_mlp_plan", [P, u8p, C.c_size_t])
+    _sig(L, "lpa_get_capable", [P, u8p, C.c_size_t])
     _sig(L, "lpa_batch_create", [C.POINTER(GraphDesc), C.c_size_t, C.POINTER(Opts), PP])
     _sig(L, "lpa_batch_run", [P, C.c_int, C.c_int, u32p])
     _sig(L, "lpa_batch_get_labels", [P, C.c_size_t, u32p, C.c_size_t])
@@ -493,6 +495,24 @@ class Propagator:
         self._chk(lib().lpa_get_learned_plan(self._h, _ptr(plan, C.c_uint8), _ptr(pred, C.c_float), k),
                   "lpa_get_learned_plan")
         return plan, pred
+
+    def mlp_plan(self) -> np.ndarray:
+        """The cost model's own plan (before the learner's trials)."""
+        k = int(self.get_info().num_segments)
+        plan = np.zeros(k, np.uint8)
+        self._chk(lib().lpa_get_mlp_plan(self._h, _ptr(plan, C.c_uint8), k), "lpa_get_mlp_plan")
+        return plan
+
+    def current_plan(self) -> np.ndarray:
+        """The variant of every segment as the next iteration will run it."""
+        return self.segments()[3]
+
+    def capable(self) -> np.ndarray:
+        """Per segment, a bit mask of the variants that can run it."""
+        k = int(self.get_info().num_segments)
+        m = np.zeros(k, np.uint8)
+        self._chk(lib().lpa_get_capable(self._h, _ptr(m, C.c_uint8), k), "lpa_get_capable")
+        return m
 
     def segment_cycles(self) -> np.ndarray:
         k = int(self.get_info().num_segments)

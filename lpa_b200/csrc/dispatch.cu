@@ -194,6 +194,7 @@ struct Learner {
   uint8_t *d_cap = nullptr, *d_var = nullptr;
   std::vector<uint8_t> cap, learned;
   std::vector<uint8_t> merged;  // the MLP's plan with every capable segment on the two-pass kernels
+  std::vector<uint8_t> mlp;     // the MLP's own plan (argmin of its predictions), before any trial
   int phase = kPhaseFixed;
   int explore_k = 0;
   int since_check = 0;
@@ -400,6 +401,7 @@ void lpa_learner_after_iteration(lpa_handle *h) {
       train(h);
       if (++L->explore_k >= kExplore) {
         infer(h);
+        L->mlp = L->learned;
         // Per-segment costs do not see a kernel's critical path or its launch:
         // the plan with the MLP's leftovers moved onto the two-pass kernels
         // is a second candidate, and the measured iteration time decides.
@@ -533,6 +535,13 @@ lpa_status lpa_get_learned_plan(lpa_handle *h, uint8_t *plan, float *pred, size_
   if (plan) std::memcpy(plan, h->learner->learned.data(), std::min(count, h->learner->learned.size()));
   if (pred && cudaMemcpy(pred, h->learner->d_pred, count * kOut * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
     return LPA_ERR_CUDA;
+  return LPA_OK;
+}
+
+lpa_status lpa_get_mlp_plan(lpa_handle *h, uint8_t *plan, size_t count) {
+  if (!h || !plan || count != h->segs.size() || !h->learner || h->learner->mlp.size() != count)
+    return LPA_ERR_INVALID_ARG;
+  std::memcpy(plan, h->learner->mlp.data(), count);
   return LPA_OK;
 }
 

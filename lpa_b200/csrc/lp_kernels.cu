@@ -751,6 +751,31 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, un
   }
 }
 
+// The block variant over one plan segment.  A vertex that one warp's table
+// and staging area hold (exact, degree <= kV1MaxDeg) is decoded and counted
+// by one warp, eight of them side by side: its 256-bit segments number at
+// most 64, so one vertex per block would leave most of the block idle while
+// a few lanes decode.  A hub (larger, or at the sketch threshold) takes the
+// whole block, whose 256 threads then decode its segments in parallel.
+__device__ void block_segment(const IterArgs &a, const Ctx &c, BlockSh &sh, uint32_t *stage, uint32_t *tab,
+                              uint32_t *wstage, unsigned long long *wslots, uint32_t &wepoch, uint32_t s,
+                              const Seg sg, bool from_scratch, unsigned long long &changed) {
+  const DevGraph &g = a.g;
+  const uint32_t t = threadIdx.x, warp = t >> 5;
+  bool fits = true;
+  for (uint32_t p = sg.begin + t; p < sg.end; p += kThreads) {
+    const uint32_t d = g.deg[p];
+    fits &= d <= kV1MaxDeg && !(a.cms_thr != 0 && d >= a.cms_thr);
+  }
+  if (__syncthreads_and(fits)) {
+    const int v = from_scratch ? kVarTwoPass : kVarWarp;
+    for (uint32_t p = sg.begin + warp; p < sg.end; p += kWarps) light_chunk(a, c, wstage, wslots, wepoch, s, p, p + 1, v, changed);
+    __syncthreads();  // the block's shared memory is free for the next item
+    return;
+  }
+  for (uint32_t p = sg.begin; p < sg.end; p++) heavy_vertex(a, c, sh, stage, tab, s, p, from_scratch, changed);
+}
+
 }  // namespace
 
 // Widens the kernel's busy span in a.ktime by this warp's start or end.
@@ -776,6 +801,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
   unsigned long long changed = 0;
   uint32_t *qctr = a.work + 4 * (a.it_dev ? c.it : 0u);
 
+  // per-warp staging and exact table of the warp-scope paths
+  unsigned long long *wslots = reinterpret_cast<unsigned long long *>(tab) + warp * kWarpSlots;
+  uint32_t *wstage = stage + warp * kWarpStage;
+  uint32_t wepoch = 0;
+
   // heavy items: one segment per block (largest first).  The next item is
   // claimed before the current one runs and its bits are prefetched into L2.
   if (t == 0) {
@@ -800,7 +830,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
     const bool from_scratch = a.seg_var[s] == kVarTwoPass;
     const Seg sg = a.segs[s];
     const long long t0 = clock64();
-    for (uint32_t p = sg.begin; p < sg.end; p++) heavy_vertex(a, c, sh, stage, tab, s, p, from_scratch, changed);
+    block_segment(a, c, sh, stage, tab, wstage, wslots, wepoch, s, sg, from_scratch, changed);
     if (a.seg_cycles && t == 0)
       atomicAdd(reinterpret_cast<unsigned long long *>(a.seg_cycles + s),
                 (unsigned long long)((clock64() - t0) * kWarps * a.cw_iterate));
@@ -808,9 +838,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
 
   // light chunks: a warp claims 4 consecutive chunks at a time, prefetches
   // the last 3 into L2 at once and runs them in order
-  unsigned long long *wslots = reinterpret_cast<unsigned long long *>(tab) + warp * kWarpSlots;
-  uint32_t *wstage = stage + warp * kWarpStage;
-  uint32_t wepoch = 0;
   for (;;) {
     uint32_t i0 = 0;
     if (lane == 0) i0 = atomicAdd(qctr + 1, 4u);
@@ -925,7 +952,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchArgs b) {
     const Seg sg = ia.segs[s];
     const int v = ia.seg_var[s];
     if (v == kVarBlock || v == kVarTwoPass) {
-      for (uint32_t p = sg.begin; p < sg.end; p++) heavy_vertex(ia, c, sh, stage, tab, s, p, false, changed);
+      block_segment(ia, c, sh, stage, tab, wstage, wslots, wepoch, s, sg, false, changed);
     } else if (v == kVarPackedLanes) {
       // a tiny segment: one thread per position (<= 256 positions)
       if (sg.begin + t < sg.end) changed += packed_vertex(ia, c, sg.begin + t);

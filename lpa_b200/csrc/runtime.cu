@@ -1121,6 +1121,17 @@ lpa_status lpa_set_plan(lpa_handle *h, const uint8_t *variant, size_t count) {
   return LPA_OK;
 }
 
+lpa_status lpa_get_capable(lpa_handle *h, uint8_t *mask, size_t count) {
+  if (!h || !mask || count != h->segs.size()) return LPA_ERR_INVALID_ARG;
+  for (size_t s = 0; s < count; s++) {
+    uint8_t m = 0;
+    for (int v = 0; v < kNumVariants; v++)
+      if (variant_capable(v, h->segs[s], h->opts.cms_threshold)) m |= uint8_t(1u << v);
+    mask[s] = m;
+  }
+  return LPA_OK;
+}
+
 lpa_status lpa_get_segments(lpa_handle *h, uint32_t *begin, uint32_t *end, uint8_t *bucket, uint8_t *variant,
                             size_t count) {
   if (!h || count != h->segs.size()) return LPA_ERR_INVALID_ARG;
