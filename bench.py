@@ -436,15 +436,18 @@ def dispatch_report(p, fixed_plan, steps: int, timed_region) -> dict:
         plan[ok] = int(v)
         plans[f"all_{v.name.lower()}"] = plan
     out = {}
+    change_ms = []
     for name, plan in plans.items():
-        p.set_plan(plan)
+        t0 = time.perf_counter()
+        p.set_plan(plan)  # the work lists are rebuilt on the device
+        change_ms.append((time.perf_counter() - t0) * 1e3)
         p.init_labels()
         ms, _ = timed_region(steps)
         out[name] = ms / steps
     static = {k: v for k, v in out.items() if k.startswith("all_")}
     best = min(static, key=static.get)
     rep = {"mlp_plan_ms": out.get("mlp_plan"), "merged_ms": out.get("merged"), "best_static_ms": static[best],
-           "best_static": best, "static_ms": static,
+           "best_static": best, "static_ms": static, "plan_change_ms": statistics.median(change_ms),
            "mlp_plan_variant_segments": [int((plans["mlp_plan"] == v).sum()) for v in range(4)]
            if "mlp_plan" in plans else None}
     return rep

@@ -13,6 +13,7 @@
 
 #include "lp_kernels.cuh"
 #include "lpa_capi.h"
+#include "plan.cuh"
 #include "runtime.h"
 
 using namespace lpa_dev;
@@ -185,150 +186,30 @@ static void build_segments(lpa_handle *h) {
   h->segs = make_segments(h->h_deg.data(), h->n, h->n_c, h->opts.cms_threshold);
 }
 
-// The device range a work item over positions [p0, p1) will read.
-static WorkItem make_item(const lpa_handle *h, uint32_t tag, uint32_t p0, uint32_t p1, bool two_pass) {
-  WorkItem w{tag, 0, 0};
-  uint64_t addr = 0, bytes = 0;
-  if (p0 < h->n_c) {
-    if (two_pass) {
-      addr = reinterpret_cast<uint64_t>(h->d_scratch + h->h_arc_off[p0]);
-      bytes = (h->h_arc_off[p1] - h->h_arc_off[p0]) * 4;
-    } else {
-      const uint64_t b = h->h_offsets[p0] >> 5, e = h->h_offsets[p1] >> 5;
-      addr = reinterpret_cast<uint64_t>(h->d_words + b);
-      bytes = (e - b + 3) * 4;
-    }
-  } else {
-    const uint64_t b = h->h_small_off[p0 - h->n_c], e = h->h_small_off[p1 - h->n_c];
-    addr = reinterpret_cast<uint64_t>(h->d_small_nbr + b);
-    bytes = (e - b) * 4;
-  }
-  w.pf_addr = addr;
-  w.pf_bytes = uint32_t(std::min<uint64_t>(bytes, 0x7FFFFFFFull));
-  return w;
-}
-
+// The plan's work lists, built on the device (plan.cu): a plan change costs a
+// few launches and one copy of the list sizes, not a host loop over n.
 static void upload_lists(lpa_handle *h) {
-  // heavy items: segments counted by a whole block (largest first); light
-  // items: 32-position chunks of the others; two-pass segments of the
-  // compressed region are decoded by the pre-pass.
-  std::vector<WorkItem> heavy, light;
-  std::vector<DecodeGroup> groups;
-  std::vector<BlockItem> cblock;
-  std::vector<PackedChunk> packed;
-  std::vector<CountItem> cwarp;
-  const uint32_t cms = h->opts.cms_threshold;
-  const uint32_t wmax = h->tune.warp_max_degree;  // above: a block item
-  // per position: 1 + the plan segment of a counted position of degree <= 32
-  std::vector<uint32_t> gmark(h->n, 0);
-  for (size_t s = 0; s < h->segs.size(); s++) {
-    const int v = h->variant[s];
-    const SegInfo &si = h->segs[s];
-    const bool tp = v == LPA_VARIANT_TWO_PASS;
-    const bool block = v == LPA_VARIANT_BLOCK || (tp && !variant_capable(LPA_VARIANT_WARP, si, h->opts.cms_threshold));
-    bool counted = false;  // two-pass positions counted by k_count_two_pass
-    if (tp) {
-      counted = true;
-      for (uint32_t p = si.begin; p < si.end; p++) {
-        const uint32_t d = h->h_deg[p];
-        if ((cms == 0 || d < cms) && d > kCountBlockMax) counted = false;  // exact above the block table
-        // the small CSR is counted by warp items only (block items read the scratch)
-        if (si.region == 1 && ((cms != 0 && d >= cms) || d > wmax)) counted = false;
-      }
-    }
-    if (counted) {
-      // runs of consecutive positions of one kind
-      uint32_t p = si.begin;
-      while (p < si.end) {
-        const uint32_t d = h->h_deg[p];
-        if (cms != 0 && d >= cms) {
-          cblock.push_back(BlockItem{h->h_arc_off[p], p, d, h->h_vertices[p], uint32_t(s), kCountSketch, 0});
-          p++;
-        } else if (d > wmax) {
-          cblock.push_back(BlockItem{h->h_arc_off[p], p, d, h->h_vertices[p], uint32_t(s), kCountBlock, 0});
-          p++;
-        } else if (d <= 32) {
-          gmark[p++] = uint32_t(s) + 1;  // group items are formed below, across segments
-        } else {
-          uint32_t q = p + 1;
-          while (q < si.end && q - p < h->tune.warp_positions) {
-            const uint32_t dq = h->h_deg[q];
-            if ((cms != 0 && dq >= cms) || dq > wmax || dq <= 32) break;
-            q++;
-          }
-          cwarp.push_back(CountItem{p, q - p, uint32_t(s), kCountWarp});
-          p = q;
-        }
-      }
-    } else if (block) {
-      heavy.push_back(make_item(h, uint32_t(s), si.begin, si.end, tp));
-    } else if (v == LPA_VARIANT_PACKED && si.max_deg <= kPackedMaxDeg) {
-      for (uint32_t p0 = si.begin; p0 < si.end; p0 += 32)
-        packed.push_back(PackedChunk{p0, std::min(si.end - p0, 32u), uint32_t(s), 0});
-    } else {
-      const uint32_t chunks = (si.end - si.begin + 31) / 32;
-      for (uint32_t c = 0; c < chunks; c++) {
-        const uint32_t p0 = si.begin + 32 * c, p1 = std::min(si.end, p0 + 32);
-        light.push_back(make_item(h, (uint32_t(s) << 3) | c, p0, p1, tp));
-      }
-    }
-    if (tp && si.region == 0) {
-      // decode groups: 32 consecutive segments of the positions, spanning at
-      // most 32 positions (every lane of the pre-pass finds its position
-      // among the 32 it loads)
-      uint32_t p = si.begin, j = 0;
-      while (p < si.end) {
-        DecodeGroup gd{p, j, 0, uint32_t(s)};
-        uint32_t positions = 0;
-        while (p < si.end && gd.nlanes < 32 && positions < 32) {
-          const uint32_t ns = h->h_nseg[p];
-          const uint32_t take = std::min(ns - j, 32u - gd.nlanes);
-          gd.nlanes += take;
-          positions++;
-          if (j + take == ns) {
-            p++;
-            j = 0;
-          } else {
-            j += take;
-          }
-        }
-        if (gd.nlanes) groups.push_back(gd);
-      }
-    }
-  }
-  std::stable_sort(heavy.begin(), heavy.end(), [&](const WorkItem &a, const WorkItem &b) {
-    return h->segs[a.tag].arcs > h->segs[b.tag].arcs;
-  });
-  // group items: up to 32 consecutive positions of one region, each either
-  // marked above or without neighbours (isolated vertices are in no segment
-  // and cut segments short; an item runs across them, since they add no
-  // arcs and keep their label).  Cycles are booked to the first position's
-  // segment.
-  for (uint64_t p = 0; p < h->n;) {
-    if (!gmark[p]) {
-      p++;
-      continue;
-    }
-    const bool reg = p >= h->n_c;
-    uint64_t q = p, last = p;
-    while (q < h->n && q - p < h->tune.group_positions && (q >= h->n_c) == reg && (gmark[q] || h->h_deg[q] == 0)) {
-      if (gmark[q]) last = q;
-      q++;
-    }
-    cwarp.push_back(CountItem{uint32_t(p), uint32_t(last + 1 - p), gmark[p] - 1, kCountGroups});
-    p = last + 1;
-  }
-  std::stable_sort(cblock.begin(), cblock.end(), [](const BlockItem &a, const BlockItem &b) { return a.d > b.d; });
-  h->n_cblock = uint32_t(cblock.size());
-  h->n_cwarp = uint32_t(cwarp.size());
-  const std::vector<CountItem> &citems = cwarp;
-  h->n_heavy = uint32_t(heavy.size());
-  h->n_light = uint32_t(light.size());
-  h->n_groups = uint32_t(groups.size());
-  std::vector<WorkItem> all;
-  all.reserve(heavy.size() + light.size());
-  all.insert(all.end(), heavy.begin(), heavy.end());
-  all.insert(all.end(), light.begin(), light.end());
+  h2d(h, h->d_seg_var, h->variant.data(), h->variant.size(), "upload variants");
+  PlanInputs in{};
+  in.segs = h->d_segdev;
+  in.nseg = uint32_t(h->segs.size());
+  in.var = h->d_seg_var;
+  in.deg = h->d_deg;
+  in.vertices = h->d_vertices;
+  in.pidx = h->d_pidx;
+  in.arc_off = h->d_arc_off;
+  in.offsets = h->d_offsets;
+  in.small_off = h->d_small_off;
+  in.words = h->d_words;
+  in.small_nbr = h->d_small_nbr;
+  in.scratch = h->d_scratch;
+  in.n = h->n;
+  in.n_c = h->n_c;
+  in.cms = h->opts.cms_threshold;
+  in.wmax = h->tune.warp_max_degree;
+  in.warp_positions = h->tune.warp_positions;
+  in.group_positions = h->tune.group_positions;
+  in.num_sms = h->num_sms;
   auto regrow = [&](auto *&ptr, size_t &cap, size_t need, const char *what) {
     if (need <= cap && ptr) return;
     if (ptr) {
@@ -339,19 +220,30 @@ static void upload_lists(lpa_handle *h) {
     cap = need + need / 4 + 16;
     ptr = dalloc<std::remove_reference_t<decltype(*ptr)>>(h, cap, what);
   };
-  regrow(h->d_items, h->items_cap, all.size(), "work items");
-  regrow(h->d_groups, h->groups_cap, groups.size(), "decode groups");
-  regrow(h->d_citems, h->citems_cap, citems.size(), "count items");
-  regrow(h->d_cblock, h->cblock_cap, cblock.size(), "count block items");
-  regrow(h->d_packed, h->packed_cap, packed.size(), "packed chunks");
-  h2d(h, h->d_packed, packed.data(), packed.size(), "upload packed chunks");
-  h->n_packed = uint32_t(packed.size());
-  h2d(h, h->d_cblock, cblock.data(), cblock.size(), "upload count block items");
-  h2d(h, h->d_citems, citems.data(), citems.size(), "upload count items");
-  h2d(h, h->d_items, all.data(), all.size(), "upload work items");
-  h2d(h, h->d_groups, groups.data(), groups.size(), "upload decode groups");
-  h2d(h, h->d_seg_var, h->variant.data(), h->variant.size(), "upload variants");
-  check(h, cudaStreamSynchronize(h->stream), "upload work lists");
+  PlanOutputs out{};
+  out.grow = [&](PlanOutputs &o) -> cudaError_t {
+    regrow(h->d_items, h->items_cap, size_t(o.n_heavy) + o.n_light, "work items");
+    regrow(h->d_groups, h->groups_cap, o.n_groups, "decode groups");
+    regrow(h->d_citems, h->citems_cap, o.n_cwarp, "count items");
+    regrow(h->d_cblock, h->cblock_cap, o.n_cblock, "count block items");
+    regrow(h->d_packed, h->packed_cap, o.n_packed, "packed chunks");
+    o.items = h->d_items;
+    o.groups = h->d_groups;
+    o.cwarp = h->d_citems;
+    o.cblock = h->d_cblock;
+    o.packed = h->d_packed;
+    return cudaSuccess;
+  };
+  std::string where;
+  const cudaError_t e = h->plan_builder.build(in, out, h->stream, where);
+  check(h, e, ("build work lists: " + where).c_str());
+  check(h, cudaStreamSynchronize(h->stream), "build work lists");
+  h->n_heavy = out.n_heavy;
+  h->n_light = out.n_light;
+  h->n_packed = out.n_packed;
+  h->n_groups = out.n_groups;
+  h->n_cblock = out.n_cblock;
+  h->n_cwarp = out.n_cwarp;
   h->plan_version++;
   // one warp per decode group, kThreads / 32 warps per block
   h->grid_decode = int(std::max<uint64_t>(
@@ -379,11 +271,6 @@ static void ensure_two_pass_scratch(lpa_handle *h) {
   }
   lpa_status st = take_device_error(h);
   if (st != LPA_OK) throw Fail{st, "position index: " + h->last_error};
-  std::vector<uint4> pidx(h->n_c);
-  if (h->n_c)
-    check(h, cudaMemcpy(pidx.data(), h->d_pidx, h->n_c * sizeof(uint4), cudaMemcpyDeviceToHost), "read index");
-  h->h_nseg.resize(h->n_c);
-  for (uint64_t p = 0; p < h->n_c; p++) h->h_nseg[p] = pidx[p].z + pidx[p].w;
   check(h, cudaStreamSynchronize(h->stream), "arc offsets");
 }
 
@@ -444,6 +331,13 @@ static void build_plan(lpa_handle *h) {
   check(h, cudaMemsetAsync(h->d_seg_changed_prev, 0, std::max<size_t>(1, ds.size()) * sizeof(uint32_t), h->stream),
         "clear segment counts");
   h2d(h, h->d_segs, ds.data(), ds.size(), "upload segments");
+  std::vector<SegDev> sd(h->segs.size());
+  for (size_t s = 0; s < h->segs.size(); s++) {
+    const SegInfo &si = h->segs[s];
+    sd[s] = SegDev{si.begin, si.end, si.max_deg, si.bucket, si.region, 0, 0, si.arcs};
+  }
+  h->d_segdev = dalloc<SegDev>(h, sd.size(), "segment table");
+  h2d(h, h->d_segdev, sd.data(), sd.size(), "upload segment table");
   check(h, cudaStreamSynchronize(h->stream), "upload segments");
   h->d_seg_cycles = dalloc<long long>(h, h->segs.size(), "segment cycles");
   h->d_ktime = dalloc<unsigned long long>(h, 2 * kBusyKernels, "kernel busy spans");
@@ -710,10 +604,6 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     for (auto &e : h->ev) check(h, cudaEventCreate(&e), "events");
     h->events_ready = true;
 
-    h->h_offsets.assign(g->offsets, g->offsets + (n_c ? n_c + 1 : 0));
-    if (n_c == 0) h->h_offsets.assign(1, 0);
-    if (n > n_c) h->h_small_off.assign(g->small_offset, g->small_offset + (n - n_c + 1));
-    h->h_vertices.assign(g->vertices, g->vertices + n_c);
     build_plan(h);
     // per-segment stream bits for the cost model's features
     for (auto &s : h->segs)
@@ -735,6 +625,7 @@ lpa_status lpa_destroy(lpa_handle *h) {
   if (!h) return LPA_ERR_INVALID_ARG;
   if (h->stream) cudaStreamSynchronize(h->stream);
   lpa_rt_destroy_graph(h);
+  h->plan_builder.release();
   for (void *p : h->allocations) cudaFree(p);
   h->allocations.clear();
   if (h->h_pinned) cudaFreeHost(h->h_pinned);

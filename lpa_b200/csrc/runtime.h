@@ -8,6 +8,7 @@
 
 #include "lp_kernels.cuh"
 #include "lpa_capi.h"
+#include "plan.cuh"
 
 namespace lpa_rt {
 
@@ -75,13 +76,14 @@ struct lpa_handle {
   std::vector<uint8_t> variant;  // per segment
   std::vector<uint8_t> fixed;    // per segment, the heuristic's choice
   lpa_dev::Seg *d_segs = nullptr;
+  lpa_dev::SegDev *d_segdev = nullptr;       // the segments as the device list builder reads them
+  lpa_dev::PlanBuilder plan_builder;         // its working memory
   uint8_t *d_seg_var = nullptr;
   lpa_dev::WorkItem *d_items = nullptr;  // heavy items | light chunk items
   lpa_dev::DecodeGroup *d_groups = nullptr;  // two-pass pre-pass work (32 segments each)
   uint32_t n_heavy = 0, n_light = 0, n_groups = 0;
   size_t items_cap = 0, groups_cap = 0;
   uint4 *d_pidx = nullptr;                   // per compressed position: section starts and segment counts
-  std::vector<uint32_t> h_nseg;              // per compressed position: interval + residual segments
   uint32_t *d_cursor = nullptr;              // per compressed position: pre-pass output cursor
   lpa_dev::CountItem *d_citems = nullptr;    // count-pass warp items
   lpa_dev::BlockItem *d_cblock = nullptr;    // count-pass block items
@@ -91,13 +93,10 @@ struct lpa_handle {
   int grid_packed = 0;
   uint32_t cw_packed = 1;
   size_t cblock_cap = 0;
-  std::vector<uint32_t> h_vertices;          // vertex id of every compressed position
   uint32_t n_cblock = 0, n_cwarp = 0;
   size_t citems_cap = 0;
   int grid_count = 0;                        // count-pass kernel
   uint32_t cw_iterate = 1, cw_decode = 1, cw_count = 1;  // seg_cycles weights (64 / resident warps per SM)
-  std::vector<uint64_t> h_offsets;        // host copies for the prefetch ranges
-  std::vector<uint32_t> h_small_off;
   std::vector<uint64_t> h_arc_off;
   int grid = 0;          // persistent iteration kernel
   int grid_decode = 0;   // two-pass decode kernel
