@@ -90,6 +90,17 @@ typedef struct lpa_opts {
    * running, before it gives up and the run returns LPA_ERR_TIMEOUT.
    * 0: the default, 2^25 (about 7 s). */
   uint64_t queue_wait_limit;
+  /* Out-of-core streaming (include/outofcore.cuh:10-96 streams CSR batches
+   * the same way).  0: the whole compressed graph resides on the device.
+   * Otherwise the bitstream stays in pinned host memory and every iteration
+   * processes the compressed positions in ranges, each range's stream words
+   * copied from host memory on a second stream while the previous range is
+   * processed.  The ranges are cut so that two stream buffers (a quarter of
+   * the budget each) and the two-pass label scratch (half) fit in this many
+   * bytes; per-vertex arrays, labels and the small CSR stay resident.
+   * LPA_ERR_CAPACITY when one vertex alone does not fit.  Single graphs only:
+   * lpa_batch_create rejects it. */
+  uint64_t stream_budget;
 } lpa_opts;
 
 typedef enum lpa_batch_mode {
@@ -122,6 +133,8 @@ typedef struct lpa_stats {
   double iterate_ms;                /* persistent iteration kernel, last iteration */
   double count_ms;                  /* two-pass count kernel, last iteration */
   double packed_ms;                 /* lane-per-vertex kernel of the tiny bucket, last iteration */
+  uint64_t stream_ranges;           /* out-of-core streaming: ranges per iteration (0: resident) */
+  uint64_t stream_bytes;            /* out-of-core streaming: stream bytes copied to the device so far */
 } lpa_stats;
 
 /* ---------------------------------------------------------------- basics -- */

@@ -106,6 +106,7 @@ class Opts(C.Structure):
         ("verbose", C.c_int),
         ("batch_mode", C.c_int),
         ("queue_wait_limit", C.c_uint64),
+        ("stream_budget", C.c_uint64),
     ]
 
 
@@ -145,6 +146,8 @@ class Stats(C.Structure):
         ("iterate_ms", C.c_double),
         ("count_ms", C.c_double),
         ("packed_ms", C.c_double),
+        ("stream_ranges", C.c_uint64),
+        ("stream_bytes", C.c_uint64),
     ]
 
 

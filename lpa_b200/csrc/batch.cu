@@ -311,6 +311,10 @@ lpa_status lpa_batch_create(const lpa_graph_desc *graphs, size_t num_graphs, con
   lpa_batch *b = new lpa_batch();
   if (o) b->opts = *o;
   else lpa_opts_default(&b->opts);
+  if (b->opts.stream_budget != 0) {  // out-of-core streaming serves single graphs only
+    delete b;
+    return LPA_ERR_INVALID_ARG;
+  }
   if (b->opts.batch_mode == LPA_BATCH_LOCKSTEP) {
     Union u;
     lpa_status st = build_union(graphs, num_graphs, u);
@@ -389,7 +393,7 @@ lpa_status lpa_batch_create(const lpa_graph_desc *graphs, size_t num_graphs, con
       if (g.num_small_arcs)
         bcheck(cudaMemcpyAsync(d_snbr + on, g.small_graph, g.num_small_arcs * 4, cudaMemcpyHostToDevice, b->stream));
       k_degree_count<<<std::max<uint64_t>(1, std::min<uint64_t>((g.num_vertices + 127) / 128, 4096)), 128, 0,
-                       b->stream>>>(bg.g, d_deg + ov, nullptr, b->d_err);
+                       b->stream>>>(bg.g, d_deg + ov, nullptr, b->d_err, 0, g.num_vertices);
       ow += g.num_words + 4;
       oo += g.num_compressed + 1;
       ov += g.num_vertices;

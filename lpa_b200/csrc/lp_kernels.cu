@@ -1730,8 +1730,8 @@ cudaError_t occupancy_count_two_pass(int *blocks) {
   return e;
 }
 
-__global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err) {
-  for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < g.n_c;
+__global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err, uint64_t p_lo, uint64_t p_hi) {
+  for (uint64_t p = p_lo + blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < p_hi;
        p += uint64_t(gridDim.x) * blockDim.x) {
     bool bad = false;
     const uint64_t o0 = g.offsets[p], end = g.offsets[p + 1];
@@ -1774,7 +1774,7 @@ __global__ void k_decode_positions(DecodeArgs a) {
   const DevGraph &g = a.g;
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < a.n_pos;
        i += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t p = a.pos_list ? a.pos_list[i] : i;
+    const uint64_t p = a.pos_list ? a.pos_list[i] : a.pos_begin + i;
     if (p >= g.n_c) continue;
     uint32_t *dst = a.out + a.arc_off[p];
     const uint64_t d = a.arc_off[p + 1] - a.arc_off[p];
@@ -1791,8 +1791,9 @@ __global__ void k_decode_positions(DecodeArgs a) {
   }
 }
 
-__global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *itv_out, uint32_t *err) {
-  for (uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < g.n;
+__global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *itv_out, uint32_t *err, uint64_t p_lo,
+                               uint64_t p_hi) {
+  for (uint64_t p = p_lo + blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; p < p_hi;
        p += uint64_t(gridDim.x) * blockDim.x) {
     uint32_t d = 0, itv = 0;
     if (g.vertices[p] >= g.n) {

@@ -217,8 +217,9 @@ cudaError_t occupancy_count_two_pass(int *blocks);
 
 struct DecodeArgs {
   DevGraph g;
-  const uint32_t *pos_list;  // positions to decode (nullptr: all of [0, n_pos))
+  const uint32_t *pos_list;  // positions to decode (nullptr: [pos_begin, pos_begin + n_pos))
   uint64_t n_pos;
+  uint64_t pos_begin;
   const uint64_t *arc_off;   // output offsets by position
   uint32_t *out;             // ids
   uint32_t *err;
@@ -227,9 +228,12 @@ __global__ void k_decode_positions(DecodeArgs a);
 
 // Per compressed position: where its interval and residual sections'
 // segments start (relative to its bit offset) and how many each has.
-__global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err);
+// Positions [p_lo, p_hi) (compressed ones only).
+__global__ void k_pos_index(DevGraph g, uint4 *pidx, uint32_t *err, uint64_t p_lo, uint64_t p_hi);
 
-__global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *itv_out, uint32_t *err);
+// Degrees (and interval items) of positions [p_lo, p_hi).
+__global__ void k_degree_count(DevGraph g, uint32_t *deg_out, uint32_t *itv_out, uint32_t *err, uint64_t p_lo,
+                               uint64_t p_hi);
 __global__ void k_init_labels(uint32_t *a, uint32_t *b, uint64_t n);
 
 }  // namespace lpa_dev

@@ -37,7 +37,7 @@ enum List : int { kLHeavy = 0, kLLight, kLPacked, kLGroups, kLBlock, kLWarp, kLi
 
 struct PlanArgs {
   const SegDev *segs;
-  uint32_t nseg;
+  uint32_t seg_begin, nseg;
   const uint8_t *var;
   const uint32_t *deg;       // by position
   const uint32_t *vertices;  // by position
@@ -48,8 +48,9 @@ struct PlanArgs {
   const uint32_t *words, *small_nbr, *scratch;
   uint64_t n, n_c;
   uint32_t cms, wmax, warp_positions, group_positions;
-  uint64_t win0;             // windows of the compressed region; the rest cover the small CSR
-  const uint32_t *off;       // kLists x (nseg + 1) exclusive offsets
+  uint64_t c_begin, c_end, s_begin, s_end;  // positions of the group items (compressed, small CSR)
+  uint64_t win0;             // windows of the compressed positions; the rest cover the small CSR
+  const uint32_t *off;       // kLists x (nseg + 1) exclusive offsets, by segment - seg_begin
   uint32_t *cnt;             // kLists x (nseg + 1) counts
   uint32_t *gmark;           // n: 1 + segment of a position counted by a group item, else 0
   uint32_t *win_cnt;         // per window: group items
@@ -94,7 +95,8 @@ __device__ WorkItem make_item(const PlanArgs &a, uint32_t tag, uint32_t p0, uint
 // One segment's items.  kEmit false: counts them (and marks the positions
 // its group items will take); true: writes them at the scanned offsets.
 template <bool kEmit>
-__device__ void plan_segment(const PlanArgs &a, uint32_t s) {
+__device__ void plan_segment(const PlanArgs &a, uint32_t i) {
+  const uint32_t s = a.seg_begin + i;
   const SegDev si = a.segs[s];
   const int v = a.var[s];
   const uint32_t cms = a.cms;
@@ -111,7 +113,7 @@ __device__ void plan_segment(const PlanArgs &a, uint32_t s) {
   uint32_t c[kLists] = {0, 0, 0, 0, 0, 0};
   uint32_t o[kLists] = {0, 0, 0, 0, 0, 0};
   if (kEmit)
-    for (int l = 0; l < kLists; l++) o[l] = a.off[l * stride + s];
+    for (int l = 0; l < kLists; l++) o[l] = a.off[l * stride + i];
   if (counted) {
     uint32_t p = si.begin;
     while (p < si.end) {
@@ -119,9 +121,10 @@ __device__ void plan_segment(const PlanArgs &a, uint32_t s) {
       const bool sk = cms != 0 && d >= cms;
       if (sk || d > a.wmax) {
         if (kEmit) {
-          const uint32_t i = o[kLBlock] + c[kLBlock];
-          a.cblock[i] = BlockItem{a.arc_off[p], p, d, a.vertices[p], s, sk ? uint32_t(kCountSketch) : uint32_t(kCountBlock), 0u};
-          a.cblock_key[i] = d;
+          const uint32_t at = o[kLBlock] + c[kLBlock];
+          a.cblock[at] = BlockItem{a.arc_off[p], p, d, a.vertices[p], s,
+                                   sk ? uint32_t(kCountSketch) : uint32_t(kCountBlock), 0u};
+          a.cblock_key[at] = d;
         }
         c[kLBlock]++;
         p++;
@@ -186,17 +189,17 @@ __device__ void plan_segment(const PlanArgs &a, uint32_t s) {
     }
   }
   if (!kEmit)
-    for (int l = 0; l < kLists; l++) a.cnt[l * stride + s] = c[l];
+    for (int l = 0; l < kLists; l++) a.cnt[l * stride + i] = c[l];
 }
 
 __global__ void k_plan_count(PlanArgs a) {
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.nseg; s += gridDim.x * blockDim.x)
-    plan_segment<false>(a, s);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nseg; i += gridDim.x * blockDim.x)
+    plan_segment<false>(a, i);
 }
 
 __global__ void k_plan_emit(PlanArgs a) {
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < a.nseg; s += gridDim.x * blockDim.x)
-    plan_segment<true>(a, s);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nseg; i += gridDim.x * blockDim.x)
+    plan_segment<true>(a, i);
 }
 
 // Group items of one window: runs of marked or isolated positions, trimmed
@@ -206,11 +209,11 @@ __device__ void plan_window(const PlanArgs &a, uint64_t w) {
   const uint64_t G = a.group_positions;
   uint64_t w0, w1;
   if (w < a.win0) {
-    w0 = w * G;
-    w1 = min(w0 + G, a.n_c);
+    w0 = a.c_begin + w * G;
+    w1 = min(w0 + G, a.c_end);
   } else {
-    w0 = a.n_c + (w - a.win0) * G;
-    w1 = min(w0 + G, a.n);
+    w0 = a.s_begin + (w - a.win0) * G;
+    w1 = min(w0 + G, a.s_end);
   }
   uint32_t k = 0;
   const uint32_t at = kEmit ? a.n_warp + a.win_off[w] : 0u;
@@ -305,7 +308,7 @@ cudaError_t PlanBuilder::build(const PlanInputs &in, PlanOutputs &out, cudaStrea
   const uint32_t S = in.nseg;
   const uint32_t stride = S + 1;
   const uint64_t G = std::max<uint32_t>(1, in.group_positions);
-  const uint64_t win0 = (in.n_c + G - 1) / G, win1 = (in.n - in.n_c + G - 1) / G;
+  const uint64_t win0 = (in.c_end - in.c_begin + G - 1) / G, win1 = (in.s_end - in.s_begin + G - 1) / G;
   const uint64_t nwin = win0 + win1;
   PB_TRY(reserve(reinterpret_cast<void **>(&cnt), cnt_cap, size_t(kLists) * stride * 4), "plan counts");
   PB_TRY(reserve(reinterpret_cast<void **>(&off), off_cap, size_t(kLists) * stride * 4), "plan offsets");
@@ -319,7 +322,12 @@ cudaError_t PlanBuilder::build(const PlanInputs &in, PlanOutputs &out, cudaStrea
 
   PlanArgs a{};
   a.segs = in.segs;
+  a.seg_begin = in.seg_begin;
   a.nseg = S;
+  a.c_begin = in.c_begin;
+  a.c_end = in.c_end;
+  a.s_begin = in.s_begin;
+  a.s_end = in.s_end;
   a.var = in.var;
   a.deg = in.deg;
   a.vertices = in.vertices;

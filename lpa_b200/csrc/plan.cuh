@@ -20,8 +20,12 @@ struct SegDev {
 };
 
 struct PlanInputs {
-  const SegDev *segs;
+  const SegDev *segs;        // every segment of the graph
+  uint32_t seg_begin;        // the lists cover segments [seg_begin, seg_begin + nseg)
   uint32_t nseg;
+  // and the count pass's group items positions [c_begin, c_end) of the
+  // compressed region and [s_begin, s_end) of the small CSR
+  uint64_t c_begin, c_end, s_begin, s_end;
   const uint8_t *var;        // variant per segment
   const uint32_t *deg;       // degree by position
   const uint32_t *vertices;  // vertex id by position

@@ -79,6 +79,39 @@ DevGraph dev_graph(const lpa_handle *h) {
   return g;
 }
 
+// ---- out-of-core streaming helpers --------------------------------------
+// Stream words that positions [p, q) read (with the 4-word tail the 64-bit
+// window may touch), from the host offsets.
+void words_of(const lpa_handle *h, const uint64_t *offsets, uint64_t p, uint64_t q, uint64_t &w0, uint64_t &w1) {
+  w0 = offsets[p] >> 5;
+  w1 = std::min<uint64_t>(((offsets[q] + 31) >> 5) + 4, h->nwords + 4);
+}
+
+// Enqueues the copy of stream words [w0, w1) into buffer b on st and returns
+// the buffer's virtual base: base[i] is stream word i for i in [w0, w1), and
+// the base itself is 16-byte aligned.
+const uint32_t *stage_words(lpa_handle *h, int b, uint64_t w0, uint64_t w1, cudaStream_t st) {
+  const uint64_t sh = w0 & 3u;
+  if (w1 - w0 + sh > h->wbuf_words) throw Fail{LPA_ERR_CAPACITY, "a stream range exceeds its buffer"};
+  check(h, cudaMemcpyAsync(h->d_wbuf[b] + sh, h->h_wpinned + w0, (w1 - w0) * 4, cudaMemcpyHostToDevice, st),
+        "stream range copy");
+  h->streamed_bytes += (w1 - w0) * 4;
+  h->wbuf_range[b] = -1;
+  return reinterpret_cast<const uint32_t *>(reinterpret_cast<uintptr_t>(h->d_wbuf[b] + sh) - uintptr_t(w0) * 4);
+}
+
+// Buffer b's virtual base for stream words starting at w0 (as stage_words
+// returns it), without copying.
+const uint32_t *words_base(const lpa_handle *h, int b, uint64_t w0) {
+  return reinterpret_cast<const uint32_t *>(reinterpret_cast<uintptr_t>(h->d_wbuf[b] + (w0 & 3u)) - uintptr_t(w0) * 4);
+}
+
+// The streamed scratch's virtual base for scratch indices [a0, ...): 16-byte
+// aligned, so the count pass's bulk copies keep their alignment.
+uint32_t *scratch_base(const lpa_handle *h, uint64_t a0) {
+  return reinterpret_cast<uint32_t *>(reinterpret_cast<uintptr_t>(h->d_scratch + (a0 & 3u)) - uintptr_t(a0) * 4);
+}
+
 void cms_seeds(uint64_t seed, uint32_t out[kCmsDepth]) {
   // seed_r = low32(seed) ^ (0x9E3779B9 * (r + 1)), plus high32(seed) * 0x85EBCA6B
   const uint32_t lo = uint32_t(seed), hi = uint32_t(seed >> 32);
@@ -188,11 +221,22 @@ static void build_segments(lpa_handle *h) {
 
 // The plan's work lists, built on the device (plan.cu): a plan change costs a
 // few launches and one copy of the list sizes, not a host loop over n.
+static void upload_range_lists(lpa_handle *h);
+
 static void upload_lists(lpa_handle *h) {
   h2d(h, h->d_seg_var, h->variant.data(), h->variant.size(), "upload variants");
+  if (h->streamed) {
+    upload_range_lists(h);
+    return;
+  }
   PlanInputs in{};
   in.segs = h->d_segdev;
+  in.seg_begin = 0;
   in.nseg = uint32_t(h->segs.size());
+  in.c_begin = 0;
+  in.c_end = h->n_c;
+  in.s_begin = h->n_c;
+  in.s_end = h->n;
   in.var = h->d_seg_var;
   in.deg = h->d_deg;
   in.vertices = h->d_vertices;
@@ -250,6 +294,83 @@ static void upload_lists(lpa_handle *h) {
       1, std::min<uint64_t>((uint64_t(h->n_groups) + kWarps - 1) / kWarps, uint64_t(h->num_sms) * 8)));
 }
 
+// The work lists of every range of a streamed handle, each built by the
+// device builder over the range's segments and positions.
+static void upload_range_lists(lpa_handle *h) {
+  auto regrow = [&](auto *&ptr, size_t &cap, size_t need, const char *what) {
+    if (need <= cap && ptr) return;
+    if (ptr) {
+      auto it = std::find(h->allocations.begin(), h->allocations.end(), (void *)ptr);
+      if (it != h->allocations.end()) h->allocations.erase(it);
+      cudaFree(ptr);
+    }
+    cap = need + need / 4 + 16;
+    ptr = dalloc<std::remove_reference_t<decltype(*ptr)>>(h, cap, what);
+  };
+  h->n_heavy = h->n_light = h->n_packed = h->n_groups = h->n_cblock = h->n_cwarp = 0;
+  for (size_t k = 0; k < h->ranges.size(); k++) {
+    StreamRange &r = h->ranges[k];
+    PlanInputs in{};
+    in.segs = h->d_segdev;
+    in.seg_begin = r.s0;
+    in.nseg = r.s1 - r.s0;
+    in.c_begin = r.p0;
+    in.c_end = r.p1;
+    in.s_begin = r.last ? h->n_c : h->n;
+    in.s_end = h->n;
+    in.var = h->d_seg_var;
+    in.deg = h->d_deg;
+    in.vertices = h->d_vertices;
+    in.pidx = h->d_pidx;
+    in.arc_off = h->d_arc_off;
+    in.offsets = h->d_offsets;
+    in.small_off = h->d_small_off;
+    in.words = words_base(h, int(k & 1), r.w0);  // prefetch ranges point into the range's buffer
+    in.small_nbr = h->d_small_nbr;
+    in.scratch = h->d_scratch ? scratch_base(h, r.a0) : nullptr;
+    in.n = h->n;
+    in.n_c = h->n_c;
+    in.cms = h->opts.cms_threshold;
+    in.wmax = h->tune.warp_max_degree;
+    in.warp_positions = h->tune.warp_positions;
+    in.group_positions = h->tune.group_positions;
+    in.num_sms = h->num_sms;
+    PlanOutputs out{};
+    out.grow = [&](PlanOutputs &o) -> cudaError_t {
+      regrow(r.items, r.items_cap, size_t(o.n_heavy) + o.n_light, "range work items");
+      regrow(r.groups, r.groups_cap, o.n_groups, "range decode groups");
+      regrow(r.cwarp, r.cwarp_cap, o.n_cwarp, "range count items");
+      regrow(r.cblock, r.cblock_cap, o.n_cblock, "range count block items");
+      regrow(r.packed, r.packed_cap, o.n_packed, "range packed chunks");
+      o.items = r.items;
+      o.groups = r.groups;
+      o.cwarp = r.cwarp;
+      o.cblock = r.cblock;
+      o.packed = r.packed;
+      return cudaSuccess;
+    };
+    std::string where;
+    const cudaError_t e = h->plan_builder.build(in, out, h->stream, where);
+    check(h, e, ("build range work lists: " + where).c_str());
+    check(h, cudaStreamSynchronize(h->stream), "build range work lists");
+    r.n_heavy = out.n_heavy;
+    r.n_light = out.n_light;
+    r.n_packed = out.n_packed;
+    r.n_groups = out.n_groups;
+    r.n_cblock = out.n_cblock;
+    r.n_cwarp = out.n_cwarp;
+    r.grid_decode = int(std::max<uint64_t>(
+        1, std::min<uint64_t>((uint64_t(r.n_groups) + kWarps - 1) / kWarps, uint64_t(h->num_sms) * 8)));
+    h->n_heavy += r.n_heavy;
+    h->n_light += r.n_light;
+    h->n_packed += r.n_packed;
+    h->n_groups += r.n_groups;
+    h->n_cblock += r.n_cblock;
+    h->n_cwarp += r.n_cwarp;
+  }
+  h->plan_version++;
+}
+
 static void ensure_two_pass_scratch(lpa_handle *h) {
   if (h->d_scratch) return;
   std::vector<uint64_t> &off = h->h_arc_off;
@@ -258,15 +379,26 @@ static void ensure_two_pass_scratch(lpa_handle *h) {
   h->d_arc_off = dalloc<uint64_t>(h, h->n + 1, "arc offsets");
   h2d(h, h->d_arc_off, off.data(), h->n + 1, "upload arc offsets");
   // + 4: a 16-byte-aligned bulk copy may read up to 12 bytes past the last label
-  h->d_scratch = dalloc<uint32_t>(h, off[h->n_c] + 4, "two-pass scratch");
+  // (streamed: one range's labels at a time, after up to 3 words of alignment)
+  h->d_scratch = dalloc<uint32_t>(h, h->streamed ? h->scratch_words : off[h->n_c] + 4, "two-pass scratch");
   // where every compressed position's segments start, for the pre-pass
   const uint64_t nc = std::max<uint64_t>(1, h->n_c);
   h->d_pidx = dalloc<uint4>(h, nc, "position index");
   h->d_cursor = dalloc<uint32_t>(h, nc, "pre-pass cursors");
   check(h, cudaMemsetAsync(h->d_cursor, 0, nc * sizeof(uint32_t), h->stream), "clear cursors");
-  if (h->n_c) {
+  if (h->streamed) {
+    for (const StreamRange &r : h->ranges) {
+      if (r.p1 <= r.p0) continue;
+      DevGraph g = dev_graph(h);
+      g.words = stage_words(h, 0, r.w0, r.w1, h->stream);
+      const int blocks = int(std::min<uint64_t>((r.p1 - r.p0 + 127) / 128, uint64_t(h->num_sms) * 32));
+      k_pos_index<<<std::max(blocks, 1), 128, 0, h->stream>>>(g, h->d_pidx, h->d_err, r.p0, r.p1);
+      check(h, cudaGetLastError(), "position index launch");
+      check(h, cudaStreamSynchronize(h->stream), "position index");  // the buffer is reused by the next range
+    }
+  } else if (h->n_c) {
     const int blocks = int(std::min<uint64_t>((h->n_c + 127) / 128, uint64_t(h->num_sms) * 32));
-    k_pos_index<<<std::max(blocks, 1), 128, 0, h->stream>>>(dev_graph(h), h->d_pidx, h->d_err);
+    k_pos_index<<<std::max(blocks, 1), 128, 0, h->stream>>>(dev_graph(h), h->d_pidx, h->d_err, 0, h->n_c);
     check(h, cudaGetLastError(), "position index launch");
   }
   lpa_status st = take_device_error(h);
@@ -287,16 +419,90 @@ static void apply_dispatch(lpa_handle *h, int dispatch, int force) {
   upload_lists(h);
 }
 
+// Ranges of a streamed handle: consecutive plan segments of the compressed
+// region whose stream fits one buffer and whose labels fit the scratch; the
+// small CSR's segments go with the last range (they read no stream).
+static void build_ranges(lpa_handle *h) {
+  const uint64_t *off = h->create_offsets;
+  std::vector<uint64_t> arc(h->n_c + 1, 0);
+  for (uint64_t p = 0; p < h->n_c; p++) arc[p + 1] = arc[p] + h->h_deg[p];
+  auto fits = [&](uint64_t p0, uint64_t p1) {
+    uint64_t w0, w1;
+    words_of(h, off, p0, p1, w0, w1);
+    return w1 - w0 + 3 <= h->wbuf_words && arc[p1] - arc[p0] + 8 <= h->scratch_words;
+  };
+  h->ranges.clear();
+  const uint32_t S = uint32_t(h->segs.size());
+  uint32_t s = 0;
+  StreamRange cur;
+  while (s < S && h->segs[s].region == 0) {
+    const SegInfo &sg = h->segs[s];
+    if (!fits(sg.begin, sg.end))
+      throw Fail{LPA_ERR_CAPACITY, "a segment's stream or labels exceed the stream budget"};
+    if (s > cur.s0 && !fits(cur.p0, sg.end)) {
+      cur.p1 = sg.begin;
+      cur.s1 = s;
+      h->ranges.push_back(cur);
+      cur = StreamRange{};
+      cur.p0 = sg.begin;
+      cur.s0 = s;
+    }
+    s++;
+  }
+  cur.p1 = h->n_c;
+  cur.s1 = S;  // the small CSR's segments too
+  cur.last = true;
+  h->ranges.push_back(cur);
+  for (StreamRange &r : h->ranges) {
+    words_of(h, off, r.p0, std::max(r.p1, r.p0), r.w0, r.w1);
+    r.a0 = arc[r.p0];
+    r.a1 = arc[r.p1];
+  }
+}
+
 static void build_plan(lpa_handle *h) {
   // degrees, decoded once on the device (validates the stream as well)
   h->d_deg = dalloc<uint32_t>(h, h->n, "degrees");
   uint32_t *d_itv = nullptr;
   check(h, cudaMalloc(&d_itv, std::max<uint64_t>(1, h->n) * sizeof(uint32_t)), "interval counts");
-  {
-    const int threads = 128;
-    const int blocks = int(std::min<uint64_t>((h->n + threads - 1) / threads, uint64_t(h->num_sms) * 32));
-    k_degree_count<<<std::max(blocks, 1), threads, 0, h->stream>>>(dev_graph(h), h->d_deg, d_itv, h->d_err);
+  const int threads = 128;
+  auto degree_pass = [&](const DevGraph &g, uint64_t p0, uint64_t p1) {
+    if (p1 <= p0) return;
+    const int blocks = int(std::min<uint64_t>((p1 - p0 + threads - 1) / threads, uint64_t(h->num_sms) * 32));
+    k_degree_count<<<std::max(blocks, 1), threads, 0, h->stream>>>(g, h->d_deg, d_itv, h->d_err, p0, p1);
     check(h, cudaGetLastError(), "degree kernel launch");
+  };
+  if (h->streamed) {
+    // compressed positions in chunks whose stream fits one buffer, then the small CSR
+    const uint64_t *off = h->create_offsets;
+    uint64_t p = 0;
+    while (p < h->n_c) {
+      uint64_t q = p + 1, w0, w1;
+      words_of(h, off, p, q, w0, w1);
+      if (w1 - w0 + 3 > h->wbuf_words) throw Fail{LPA_ERR_CAPACITY, "a vertex's stream exceeds the stream budget"};
+      uint64_t step = 1;
+      while (q < h->n_c) {  // grow the chunk by doubling steps, then halving
+        const uint64_t t = std::min<uint64_t>(h->n_c, q + step);
+        words_of(h, off, p, t, w0, w1);
+        if (w1 - w0 + 3 <= h->wbuf_words) {
+          q = t;
+          step *= 2;
+        } else if (step > 1) {
+          step /= 2;
+        } else {
+          break;
+        }
+      }
+      words_of(h, off, p, q, w0, w1);
+      DevGraph g = dev_graph(h);
+      g.words = stage_words(h, 0, w0, w1, h->stream);
+      degree_pass(g, p, q);
+      check(h, cudaStreamSynchronize(h->stream), "degree pass");  // the buffer is reused by the next chunk
+      p = q;
+    }
+    degree_pass(dev_graph(h), h->n_c, h->n);
+  } else {
+    degree_pass(dev_graph(h), 0, h->n);
   }
   lpa_status st = take_device_error(h);
   if (st != LPA_OK) throw Fail{st, "degree pass: " + h->last_error};
@@ -318,6 +524,7 @@ static void build_plan(lpa_handle *h) {
     for (uint32_t p = sg.begin; p < sg.end; p++) iv += itv[p];
     sg.intervals = uint32_t(std::min<uint64_t>(iv, 0xFFFFFFFFull));
   }
+  if (h->streamed) build_ranges(h);
   h->fixed.resize(h->segs.size());
   for (size_t s = 0; s < h->segs.size(); s++) h->fixed[s] = uint8_t(fixed_variant(h->segs[s]));
   std::vector<Seg> ds(h->segs.size());
@@ -413,7 +620,13 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
 // Enqueues one iteration (no host synchronisation).  Swaps the buffers.  The
 // changed counter and the two queue counters of the iteration's slot must be
 // zero.
+static void enqueue_streamed_iteration(lpa_handle *h, unsigned long long *changed, uint32_t *work);
+
 static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32_t *work) {
+  if (h->streamed) {
+    enqueue_streamed_iteration(h, changed, work);
+    return;
+  }
   const bool timed = h->opts.record_timings && h->events_ready;
   const IterArgs a = iter_args(h, changed, work);
   // events only around the kernels that run: an event costs a few us of
@@ -453,6 +666,86 @@ static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32
   h->cur ^= 1;
 }
 
+// One iteration of a streamed handle: range by range, each range's stream
+// words copied on the copy stream into one of two buffers (the copy of range
+// k + 1 overlaps the kernels of range k), its kernels then launched on the
+// handle's stream over its own work lists with the buffer's and the scratch's
+// virtual bases.  A buffer that still holds its range's words (two ranges or
+// fewer) is not copied again.  Every range reads the same label buffer and
+// writes the other; the buffers swap once, after the last range.
+static void enqueue_streamed_iteration(lpa_handle *h, unsigned long long *changed, uint32_t *work) {
+  const bool timed = h->opts.record_timings && h->events_ready;
+  if (timed) {
+    h->ev_kernel[0] = -1;
+    cudaEventRecord(h->ev[0], h->stream);
+  }
+  const size_t R = h->ranges.size();
+  std::vector<const uint32_t *> base(R, nullptr);
+  auto issue_copy = [&](size_t k) {
+    const StreamRange &r = h->ranges[k];
+    const int b = int(k & 1);
+    if (h->wbuf_range[b] == int(k)) {
+      base[k] = words_base(h, b, r.w0);
+      return;
+    }
+    check(h, cudaStreamWaitEvent(h->copy_stream, h->ev_free[b], 0), "wait for a free stream buffer");
+    base[k] = stage_words(h, b, r.w0, r.w1, h->copy_stream);
+    check(h, cudaEventRecord(h->ev_ready[b], h->copy_stream), "stream buffer ready");
+    h->wbuf_range[b] = int(k);
+  };
+  if (R) issue_copy(0);
+  for (size_t k = 0; k < R; k++) {
+    if (k + 1 < R) issue_copy(k + 1);
+    const StreamRange &r = h->ranges[k];
+    const int b = int(k & 1);
+    check(h, cudaStreamWaitEvent(h->stream, h->ev_ready[b], 0), "wait for the stream range");
+    IterArgs a = iter_args(h, changed, work + 4 * k);
+    a.g.words = base[k];
+    a.heavy = r.items;
+    a.n_heavy = r.n_heavy;
+    a.light = r.items + r.n_heavy;
+    a.n_light = r.n_light;
+    a.groups = r.groups;
+    a.n_groups = r.n_groups;
+    a.cblock = r.cblock;
+    a.n_cblock = r.n_cblock;
+    a.cwarp = r.cwarp;
+    a.n_cwarp = r.n_cwarp;
+    a.packed = r.packed;
+    a.n_packed = r.n_packed;
+    a.scratch = h->d_scratch ? scratch_base(h, r.a0) : nullptr;
+    if (r.n_groups) {
+      launch_decode_two_pass(h->tune.gather_cache, r.grid_decode, h->stream, a);
+      h->launches++;
+    }
+    if (r.n_cblock + r.n_cwarp) {
+      launch_count_two_pass(h->tune.bulk_stage != 0, h->grid_count, h->stream, a);
+      h->launches++;
+    }
+    if (r.n_packed) {
+      k_packed<<<h->grid_packed, kThreads, 0, h->stream>>>(a);
+      h->launches++;
+    }
+    if (r.n_heavy + r.n_light) {
+      k_iterate<<<h->grid, kThreads, kSmemBytes, h->stream>>>(a);
+      h->launches++;
+    }
+    check(h, cudaEventRecord(h->ev_free[b], h->stream), "stream buffer free");
+  }
+  if (h->d_gtrack) {
+    lpa_rt_enqueue_track(h);
+    h->launches += 2;
+  }
+  if (timed) {
+    h->ev_kernel[1] = -1;  // the whole iteration: no per-kernel split
+    cudaEventRecord(h->ev[1], h->stream);
+    h->ev_used = 2;
+  } else {
+    h->ev_used = 0;
+  }
+  h->cur ^= 1;
+}
+
 static void collect_times(lpa_handle *h) {
   if (!(h->opts.record_timings && h->events_ready)) return;
   auto ms = [&](int a, int b) {
@@ -465,7 +758,8 @@ static void collect_times(lpa_handle *h) {
   };
   for (int v = 0; v < 4; v++) h->variant_ms[v] = 0;
   double k_ms[4] = {0, 0, 0, 0};  // pre-pass, count pass, k_packed, k_iterate
-  for (int e = 1; e < h->ev_used; e++) k_ms[h->ev_kernel[e]] = ms(e - 1, e);
+  for (int e = 1; e < h->ev_used; e++)
+    if (h->ev_kernel[e] >= 0 && h->ev_kernel[e] < 4) k_ms[h->ev_kernel[e]] = ms(e - 1, e);
   h->decode_ms = k_ms[0];
   h->count_ms = k_ms[1];
   h->packed_ms = k_ms[2];
@@ -578,9 +872,27 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
 
     // device copies; the stream gets 4 zero words of tail for the 64-bit window
     const uint64_t wcount = h->nwords + 4;
-    h->d_words = dalloc<uint32_t>(h, wcount, "bitstream");
-    check(h, cudaMemsetAsync(h->d_words, 0, wcount * sizeof(uint32_t), h->stream), "clear bitstream");
-    h2d(h, h->d_words, g->words, h->nwords, "upload bitstream");
+    h->streamed = h->opts.stream_budget != 0 && n_c != 0;
+    if (h->streamed) {
+      // out of core: the stream in pinned host memory, two device buffers of
+      // a quarter of the budget each, the label scratch in the other half
+      h->wbuf_words = h->opts.stream_budget / 16;
+      h->scratch_words = h->opts.stream_budget / 8;
+      if (h->wbuf_words < 64 || h->scratch_words < 64) throw Fail{LPA_ERR_INVALID_ARG, "stream budget too small"};
+      check(h, cudaMallocHost(&h->h_wpinned, wcount * sizeof(uint32_t)), "pinned stream");
+      std::memcpy(h->h_wpinned, g->words, h->nwords * sizeof(uint32_t));
+      std::memset(h->h_wpinned + h->nwords, 0, 4 * sizeof(uint32_t));
+      for (int b = 0; b < 2; b++) h->d_wbuf[b] = dalloc<uint32_t>(h, h->wbuf_words, "stream buffer");
+      check(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking), "copy stream");
+      for (int b = 0; b < 2; b++) {
+        check(h, cudaEventCreateWithFlags(&h->ev_ready[b], cudaEventDisableTiming), "events");
+        check(h, cudaEventCreateWithFlags(&h->ev_free[b], cudaEventDisableTiming), "events");
+      }
+    } else {
+      h->d_words = dalloc<uint32_t>(h, wcount, "bitstream");
+      check(h, cudaMemsetAsync(h->d_words, 0, wcount * sizeof(uint32_t), h->stream), "clear bitstream");
+      h2d(h, h->d_words, g->words, h->nwords, "upload bitstream");
+    }
     h->d_offsets = dalloc<uint64_t>(h, n_c + 1, "offsets");
     if (n_c) h2d(h, h->d_offsets, g->offsets, n_c + 1, "upload offsets");
     h->d_vertices = dalloc<uint32_t>(h, n, "vertices");
@@ -604,7 +916,9 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     for (auto &e : h->ev) check(h, cudaEventCreate(&e), "events");
     h->events_ready = true;
 
+    h->create_offsets = g->offsets;
     build_plan(h);
+    h->create_offsets = nullptr;
     // per-segment stream bits for the cost model's features
     for (auto &s : h->segs)
       if (s.region == 0) s.bits = g->offsets[s.end] - g->offsets[s.begin];
@@ -629,6 +943,13 @@ lpa_status lpa_destroy(lpa_handle *h) {
   for (void *p : h->allocations) cudaFree(p);
   h->allocations.clear();
   if (h->h_pinned) cudaFreeHost(h->h_pinned);
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  if (h->h_wpinned) cudaFreeHost(h->h_wpinned);
+  for (int b = 0; b < 2; b++) {
+    if (h->ev_ready[b]) cudaEventDestroy(h->ev_ready[b]);
+    if (h->ev_free[b]) cudaEventDestroy(h->ev_free[b]);
+  }
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   for (auto &e : h->ev)
     if (e) cudaEventDestroy(e);
   lpa_learner_free(h);
@@ -701,7 +1022,8 @@ lpa_status lpa_iterate(lpa_handle *h, uint64_t *changed_out) {
     lpa_learner_before_iteration(h);
     unsigned long long *slot = h->d_changed;
     check(h, cudaMemsetAsync(slot, 0, sizeof(unsigned long long), h->stream), "clear counter");
-    check(h, cudaMemsetAsync(h->d_work, 0, 4 * sizeof(uint32_t), h->stream), "clear work counters");
+    const size_t slots = h->streamed ? std::max<size_t>(1, h->ranges.size()) : 1;  // a counter block per range
+    check(h, cudaMemsetAsync(h->d_work, 0, 4 * slots * sizeof(uint32_t), h->stream), "clear work counters");
     enqueue_iteration(h, slot, h->d_work);
     check(h, cudaGetLastError(), "iteration launch");
     check(h, cudaMemcpyAsync(h->h_pinned, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream),
@@ -738,6 +1060,17 @@ lpa_status lpa_run(lpa_handle *h, int max_iter, int early_exit, int *iters_done)
       return LPA_OK;
     }
   }
+  if (h->streamed) {  // the copies of the ranges run from the host loop
+    while (done < max_iter) {
+      uint64_t ch = 0;
+      lpa_status st = lpa_iterate(h, &ch);
+      if (st != LPA_OK) return st;
+      done++;
+      if (early_exit && ch == 0) break;
+    }
+    if (iters_done) *iters_done = done;
+    return LPA_OK;
+  }
   int rest = 0;
   lpa_status st = lpa_run_graph(h, max_iter - done, early_exit != 0, &rest);
   if (iters_done) *iters_done = done + rest;
@@ -772,6 +1105,8 @@ lpa_status lpa_get_stats(lpa_handle *h, lpa_stats *st) {
   st->last_iter_ms = h->last_iter_ms;
   st->launches = h->launches;
   st->decode_ms = h->decode_ms;
+  st->stream_ranges = h->streamed ? h->ranges.size() : 0;
+  st->stream_bytes = h->streamed_bytes;
   st->iterate_ms = h->iterate_ms;
   st->count_ms = h->count_ms;
   st->packed_ms = h->packed_ms;
@@ -795,23 +1130,40 @@ lpa_status lpa_decode_csr(lpa_handle *h, uint64_t *row_out, uint32_t *clm_out) {
   try {
     check(h, cudaSetDevice(h->device), "cudaSetDevice");
     ensure_two_pass_scratch(h);
-    DecodeArgs a{};
-    a.g = dev_graph(h);
-    a.pos_list = nullptr;
-    a.n_pos = h->n_c;
-    a.arc_off = h->d_arc_off;
-    a.out = h->d_scratch;
-    a.err = h->d_err;
-    const int blocks = int(std::max<uint64_t>(1, std::min<uint64_t>((h->n_c + 255) / 256, uint64_t(h->num_sms) * 8)));
-    if (h->n_c) k_decode_positions<<<blocks, 256, 0, h->stream>>>(a);
-    check(h, cudaGetLastError(), "decode launch");
-    lpa_status st = take_device_error(h);
-    if (st != LPA_OK) return st;
     std::vector<uint64_t> off(h->n + 1, 0);
     for (uint64_t p = 0; p < h->n; p++) off[p + 1] = off[p] + h->h_deg[p];
     std::vector<uint32_t> ids(off[h->n_c]);
+    DecodeArgs a{};
+    a.g = dev_graph(h);
+    a.pos_list = nullptr;
+    a.arc_off = h->d_arc_off;
+    a.err = h->d_err;
+    auto decode = [&](uint64_t p0, uint64_t p1) {
+      a.pos_begin = p0;
+      a.n_pos = p1 - p0;
+      const int blocks = int(std::max<uint64_t>(1, std::min<uint64_t>((a.n_pos + 255) / 256, uint64_t(h->num_sms) * 8)));
+      if (a.n_pos) k_decode_positions<<<blocks, 256, 0, h->stream>>>(a);
+      check(h, cudaGetLastError(), "decode launch");
+      return take_device_error(h);
+    };
+    if (h->streamed) {  // range by range through one stream buffer and the scratch
+      for (const StreamRange &r : h->ranges) {
+        if (r.p1 <= r.p0) continue;
+        a.g.words = stage_words(h, 0, r.w0, r.w1, h->stream);
+        a.out = scratch_base(h, r.a0);
+        lpa_status st = decode(r.p0, r.p1);
+        if (st != LPA_OK) return st;
+        if (r.a1 > r.a0)
+          check(h, cudaMemcpy(ids.data() + r.a0, h->d_scratch + (r.a0 & 3u), (r.a1 - r.a0) * 4, cudaMemcpyDeviceToHost),
+                "read decode");
+      }
+    } else {
+      a.out = h->d_scratch;
+      lpa_status st = decode(0, h->n_c);
+      if (st != LPA_OK) return st;
+      check(h, cudaMemcpy(ids.data(), h->d_scratch, ids.size() * 4, cudaMemcpyDeviceToHost), "read decode");
+    }
     std::vector<uint32_t> verts(h->n);
-    check(h, cudaMemcpy(ids.data(), h->d_scratch, ids.size() * 4, cudaMemcpyDeviceToHost), "read decode");
     check(h, cudaMemcpy(verts.data(), h->d_vertices, h->n * 4, cudaMemcpyDeviceToHost), "read vertices");
     std::vector<uint32_t> sm_off(h->n - h->n_c + 1, 0), sm_nbr(h->m_small);
     if (h->n > h->n_c)
@@ -868,7 +1220,8 @@ static double tune_trial(lpa_handle *h, int repeats) {
     check(h, cudaMemsetAsync(h->d_ktime + kBusyKernels, 0, kBusyKernels * sizeof(unsigned long long), h->stream),
           "clear spans");
     check(h, cudaMemsetAsync(h->d_changed, 0, sizeof(unsigned long long), h->stream), "clear counter");
-    check(h, cudaMemsetAsync(h->d_work, 0, 4 * sizeof(uint32_t), h->stream), "clear work counters");
+    const size_t slots = h->streamed ? std::max<size_t>(1, h->ranges.size()) : 1;
+    check(h, cudaMemsetAsync(h->d_work, 0, 4 * slots * sizeof(uint32_t), h->stream), "clear work counters");
     enqueue_iteration(h, h->d_changed, h->d_work);
     h->cur = cur;
     check(h, cudaGetLastError(), "tuning iteration");

@@ -46,6 +46,26 @@ std::vector<SegInfo> make_segments(const uint32_t *deg, uint64_t n, uint64_t n_c
 
 }  // namespace lpa_rt
 
+// One range of an out-of-core (streamed) handle: compressed positions
+// [p0, p1) and the plan segments [s0, s1) inside them (the last range also
+// takes the small CSR's segments), the stream words [w0, w1) they read and
+// their two-pass scratch indices [a0, a1), with the range's own work lists.
+struct StreamRange {
+  uint64_t p0 = 0, p1 = 0;
+  uint32_t s0 = 0, s1 = 0;
+  uint64_t w0 = 0, w1 = 0;
+  uint64_t a0 = 0, a1 = 0;
+  bool last = false;
+  lpa_dev::WorkItem *items = nullptr;
+  lpa_dev::PackedChunk *packed = nullptr;
+  lpa_dev::DecodeGroup *groups = nullptr;
+  lpa_dev::BlockItem *cblock = nullptr;
+  lpa_dev::CountItem *cwarp = nullptr;
+  size_t items_cap = 0, packed_cap = 0, groups_cap = 0, cblock_cap = 0, cwarp_cap = 0;
+  uint32_t n_heavy = 0, n_light = 0, n_packed = 0, n_groups = 0, n_cblock = 0, n_cwarp = 0;
+  int grid_decode = 1;
+};
+
 struct lpa_handle {
   lpa_opts opts{};
   lpa_tune tune{32, 4, lpa_dev::kCountWarpMax, 2, 0, 0};  // count-pass work shapes (lpa_set_tune / lpa_autotune)
@@ -129,6 +149,20 @@ struct lpa_handle {
   bool events_ready = false;
   uint64_t device_bytes = 0;
   std::vector<void *> allocations;
+
+  // out-of-core streaming (opts.stream_budget): the stream in pinned host
+  // memory, two device buffers filled on copy_stream, the ranges
+  bool streamed = false;
+  uint32_t *h_wpinned = nullptr;
+  uint32_t *d_wbuf[2] = {nullptr, nullptr};
+  uint64_t wbuf_words = 0;     // capacity of each buffer (words)
+  uint64_t scratch_words = 0;  // capacity of the streamed scratch (words)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_ready[2] = {}, ev_free[2] = {};
+  std::vector<StreamRange> ranges;
+  uint64_t streamed_bytes = 0;  // stream bytes copied host -> device so far
+  int wbuf_range[2] = {-1, -1};  // the range whose words each buffer holds (-1: none)
+  const uint64_t *create_offsets = nullptr;  // the caller's bit offsets, during lpa_create only
 
   // CUDA-graph loop: while set, kernels take their parity and counter slot from it
   const uint32_t *loop_it = nullptr;
