@@ -46,7 +46,8 @@ WORKLOADS = {
     "rmat-s22": dict(kind="rmat", scale=22, edge_factor=16.0, seed=1, small_thresh=32, cms=1024, iters=20),
     # web-like copy model: 100M vertices, out-degree 30 (prototype copies p=0.6 with
     # offsets in [-8,8], else Zipf(1.1) targets); threshold 16, sketch >= 4096
-    "copy-100m": dict(kind="copy", n=100_000_000, out_degree=30, seed=1, small_thresh=16, cms=4096, iters=10),
+    "copy-100m": dict(kind="copy", n=100_000_000, out_degree=30, seed=1, small_thresh=16, cms=4096, iters=10,
+                      loop="graph"),
     # many uneven graphs in one persistent launch: vertex counts log-uniform in
     # [1k, 256k], even graphs road grids (p=0.7), odd graphs R-MAT (edge factor 8),
     # threshold 16, per-graph early exit (the 4096-graph [1k, 2M] batch scaled down)
@@ -486,6 +487,9 @@ def main():
     ap.add_argument("--batch-mode", default="lockstep", choices=["lockstep", "queue"],
                     help="batched workloads: the concatenated graph in lockstep, or the persistent queue")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--loop", choices=["host", "graph"], default=None,
+                    help="host: one lpa_iterate per step; graph: the timed steps in one lpa_run (CUDA-graph loop); "
+                         "default per workload (graph for copy-100m)")
     ap.add_argument("--no-dispatch-report", dest="dispatch_report", action="store_false",
                     help="skip timing the cost model's own plan and the single-variant plans after the run")
     args = ap.parse_args()
@@ -530,8 +534,25 @@ def main():
     flush = inputs_bytes < 2 * L2_BYTES
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=device) if flush else None
 
+    loop = args.loop or w.get("loop", "host")
+    if loop == "graph" and flush:
+        raise SystemExit("--loop graph needs inputs larger than L2 (no flush fits inside the graph)")
+
     def timed_region(steps):
-        """K iterations; device time of each from the library's CUDA events."""
+        """K iterations; device time of each from the library's CUDA events,
+        or with the CUDA-graph loop one lpa_run call of K iterations (the
+        iteration kernels and the device-side loop test in a conditional
+        node), timed by CUDA events on the library's stream around it."""
+        if loop == "graph":
+            p.run(1)  # the graph is (re)built for the current plan outside the timing
+            p.init_labels()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            done = p.run(steps, early_exit=False)
+            e1.record(stream)
+            e1.synchronize()
+            assert done == steps
+            return e0.elapsed_time(e1), np.full(4, np.nan)
         dev = 0.0
         kern = np.zeros(4)
         for _ in range(steps):
@@ -639,6 +660,7 @@ def main():
                        "stream_bytes": (int(info.stream_bits) + 7) // 8, "small_thresh": w["small_thresh"],
                        "cms_threshold": w["cms"], "dispatch": args.dispatch,
                        "timed_iterations": f"1..{args.steps} from the initial labels",
+                       "loop": "CUDA-graph loop (lpa_run)" if loop == "graph" else "host loop (lpa_iterate per step)",
                        "l2": "L2 flushed between iterations" if flush else "inputs larger than L2",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm",
@@ -647,8 +669,9 @@ def main():
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "bytes_per_launch": b_alg, "ms_per_launch": ms_per_step,
                          "traffic": traffic_summary(args.workload),
-                         "kernel_ms": {"k_decode_two_pass": float(kern_avg[0]), "k_count_two_pass": float(kern_avg[1]),
-                                       "k_packed": float(kern_avg[2]), "k_iterate": float(kern_avg[3])}},
+                         "kernel_ms": None if loop == "graph" else
+                         {"k_decode_two_pass": float(kern_avg[0]), "k_count_two_pass": float(kern_avg[1]),
+                          "k_packed": float(kern_avg[2]), "k_iterate": float(kern_avg[3])}},
             "dispatch": {"mode": args.dispatch,
                          "fixed_value": arcs * args.steps * world / (fixed_ms / 1e3),
                          "fixed_ms_per_step": fixed_ms / args.steps,

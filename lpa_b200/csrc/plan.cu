@@ -101,7 +101,11 @@ __device__ void plan_segment(const PlanArgs &a, uint32_t i) {
   const int v = a.var[s];
   const uint32_t cms = a.cms;
   const bool tp = v == kVarTwoPass;
-  const bool block = v == kVarBlock || (tp && !warp_capable(si, cms));
+  // a block-variant segment whose vertices one warp holds runs as warp
+  // chunks (one vertex per warp at a time, k_iterate's light loop) instead of
+  // one vertex per block: its vertices have at most 64 segments of 256 bits,
+  // too few to keep a block busy, and block items wait at barriers
+  const bool block = (v == kVarBlock || tp) && !warp_capable(si, cms);
   bool counted = tp;  // the two-pass count pass takes the segment's positions
   if (tp) {
     // exact above the count pass's block table (a hub is alone in its segment)
