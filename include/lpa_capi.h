@@ -204,6 +204,11 @@ typedef struct lpa_tune {
   uint32_t gather_cache;     /* cache path of the two-pass pre-pass's label reads: 0 (default) the labels
                                 of the lowest n/64 ids through L1, the rest through L2 only; 1 all through
                                 L2 only, leaving L1 to the bitstream; 2 all through L1 (hot labels) */
+  uint32_t stage_stream;     /* how the pre-pass moves each decode group's stream span ahead of its decode:
+                                0 (default) not at all (per-lane loads); 1 a bulk prefetch of the next
+                                group's span into L2; 2 a bulk copy of the next group's span into one of
+                                the warp's two shared-memory buffers (mbarrier-completed), overlapping the
+                                current group's decode */
 } lpa_tune;
 lpa_status lpa_get_tune(struct lpa_handle *h, lpa_tune *out);
 /* Installs the knobs (out of range: LPA_ERR_INVALID_ARG) and rebuilds the work lists. */

@@ -73,11 +73,12 @@ class Tune(C.Structure):
         ("warp_claim", C.c_uint32),
         ("bulk_stage", C.c_uint32),
         ("gather_cache", C.c_uint32),
+        ("stage_stream", C.c_uint32),
     ]
 
     def as_tuple(self):
         return (self.group_positions, self.warp_positions, self.warp_max_degree, self.warp_claim, self.bulk_stage,
-                self.gather_cache)
+                self.gather_cache, self.stage_stream)
 
 
 class GraphDesc(C.Structure):
@@ -481,8 +482,9 @@ class Propagator:
         self._chk(lib().lpa_get_tune(self._h, C.byref(t)), "lpa_get_tune")
         return t
 
-    def set_tune(self, group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage=0, gather_cache=0):
-        t = Tune(group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage, gather_cache)
+    def set_tune(self, group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage=0, gather_cache=0,
+                 stage_stream=0):
+        t = Tune(group_positions, warp_positions, warp_max_degree, warp_claim, bulk_stage, gather_cache, stage_stream)
         self._chk(lib().lpa_set_tune(self._h, C.byref(t)), "lpa_set_tune")
 
     def autotune(self, cache_path=None, repeats=2) -> Tune:

@@ -55,7 +55,23 @@ __device__ __forceinline__ uint64_t win64(W w, uint64_t pos) {
 // Global-memory word source (read-only path).
 struct GWords {
   const uint32_t *__restrict__ p;
+  GWords() = default;
+  __device__ __forceinline__ GWords(const uint32_t *q) : p(q) {}
   __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return __ldg(p + i); }
+};
+
+// Words [lo, lo + n) from a shared-memory copy, every other word from global
+// memory: a reader whose span was staged reads the copy, and anything outside
+// the staged span (a clipped copy, a malformed stream) still reads the stream.
+struct StagedWords {
+  const uint32_t *__restrict__ g;  // the stream (global memory)
+  const uint32_t *s;               // shared copy of words [lo, lo + n)
+  uint64_t lo;
+  uint32_t n;
+  __device__ __forceinline__ uint32_t operator()(uint64_t i) const {
+    const uint64_t k = i - lo;
+    return k < n ? s[k] : __ldg(g + i);
+  }
 };
 
 // Shared-memory word source: words [base_word, base_word + len) staged at s.
@@ -217,8 +233,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
   return false;
 }
 
-struct BitReader {
-  const uint32_t *__restrict__ w;
+// WS: the word source (GWords, or StagedWords for a span staged in shared
+// memory).
+template <class WS>
+struct BitReaderT {
+  WS w;
   uint32_t hi, lo;  // upcoming bits, MSB-aligned: hi the next 32, lo the 32 after (zero past the valid bits)
   uint64_t wnext;   // next word to load
   uint32_t nb;      // valid bits in hi:lo
@@ -226,11 +245,11 @@ struct BitReader {
   // absolute position of the next unread bit (kept implicit: every code
   // would otherwise pay a 64-bit add)
   __device__ __forceinline__ uint64_t pos() const { return (wnext << 5) - nb; }
-  __device__ __forceinline__ void seek(const uint32_t *__restrict__ words, uint64_t p) {
+  __device__ __forceinline__ void seek(WS words, uint64_t p) {
     w = words;
     const uint64_t i = p >> 5;
     const uint32_t s = uint32_t(p) & 31u;
-    const uint32_t a = __ldg(w + i), b = __ldg(w + i + 1);
+    const uint32_t a = w(i), b = w(i + 1);
     hi = __funnelshift_l(b, a, s);
     lo = b << s;
     nb = 64 - s;
@@ -239,7 +258,7 @@ struct BitReader {
   // Tops the buffer up to at least 33 valid bits (from at least 1).
   __device__ __forceinline__ void fill() {
     if (nb <= 32) {  // every valid bit is in hi and lo is zero
-      const uint32_t x = __ldg(w + wnext);
+      const uint32_t x = w(wnext);
       hi |= __funnelshift_rc(x, 0u, nb);  // x >> nb, 0 when nb == 32
       lo = x << (32 - nb);
       wnext++;
@@ -263,7 +282,7 @@ struct BitReader {
       return v - 1u;
     }
     uint64_t p = pos();
-    const uint32_t v = dec_gamma(GWords{w}, p, bad);
+    const uint32_t v = dec_gamma(w, p, bad);
     seek(w, p);
     return v;
   }
@@ -276,7 +295,7 @@ struct BitReader {
       return v - 1u;
     }
     uint64_t p = pos();
-    const uint32_t v = dec_zeta3(GWords{w}, p, bad);
+    const uint32_t v = dec_zeta3(w, p, bad);
     seek(w, p);
     return v;
   }
@@ -293,6 +312,7 @@ struct BitReader {
     return gamma(bad) + 1u;
   }
 };
+using BitReader = BitReaderT<GWords>;
 
 // Walks one vertex with the buffered reader (same contract as walk_vertex).
 template <class Emit>

@@ -19,6 +19,8 @@
 //     several vertices per round for degrees <= 32).
 // Every loop is bounded by the bits it consumes; malformed input sets the
 // error word instead of trapping.
+#include <type_traits>
+
 #include "lp_kernels.cuh"
 #include "noalloc.cuh"
 
@@ -1082,19 +1084,91 @@ __global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
 // 0 the labels of the lowest n/64 ids through L1 and the rest through L2
 // only, which on R-MAT and the copy model comes within 0.5 % of the better
 // of the two.
-template <int kGather>
+//
+// kStage (lpa_tune.stage_stream) moves each group's stream span (the words its
+// segments read, DecodeGroup::w0/wn) ahead of its decode with the copy
+// engine: 1 a bulk prefetch of the next group's span into L2
+// (cp.async.bulk.prefetch.L2) while the warp decodes the current one; 2 a 1-D
+// bulk copy of the next group's span into one of two shared-memory buffers of
+// the warp (cp.async.bulk ... mbarrier::complete_tx, 16-byte aligned, no
+// multicast), completed on that buffer's mbarrier with a bounded wait, so the
+// copy of group k + 1 overlaps the decode of group k; the lanes then read
+// their words from the buffer (words outside the copied span, if any, from
+// the stream itself).
+template <int kGather, int kStage>
 __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   __shared__ uint32_t stage[kWarps * kDecodeWindow];
   __shared__ uint8_t owner[kWarps * kDecodeWindow];
+  extern __shared__ __align__(16) uint32_t sspan[];  // kStage 2: kSpanSmemBytes of dynamic shared memory
+  __shared__ uint64_t sbar[kStage == 2 ? kWarps * 2 : 1];
+  using WS = typename std::conditional<kStage == 2, StagedWords, GWords>::type;
   const DevGraph &g = a.g;
   const Ctx c = resolve(a);
   const uint32_t hot = uint32_t(g.n >> 6);  // kGather 0: ids below read through L1
   busy_mark(a, 0, false);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t gi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gi < a.n_groups; gi += nw) {
+  const uint32_t gfirst = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t *wspan = sspan + (kStage == 2 ? warp * 2 * kSpanWords : 0);
+  uint64_t *wbar = sbar + (kStage == 2 ? warp * 2 : 0);
+  uint32_t phase[2] = {0u, 0u};
+  // the words [lo, lo + n) of group gi's span that buffer b receives
+  const auto span_of = [&](const DecodeGroup &d, uint64_t &lo, uint32_t &n) {
+    lo = d.w0 & ~uint64_t(3);
+    const uint64_t hi = min(min(d.w0 + d.wn, a.wend), lo + kSpanWords);
+    n = hi > lo ? uint32_t((hi - lo) & ~uint64_t(3)) : 0u;
+  };
+  const auto issue = [&](uint32_t gi, uint32_t b) {  // lane 0
+    const DecodeGroup d = a.groups[gi];
+    uint64_t lo;
+    uint32_t n;
+    span_of(d, lo, n);
+    if (n) bulk_load(wspan + b * kSpanWords, g.words + lo, n * 4u, wbar + b);
+    else asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(wbar + b)) : "memory");
+  };
+  if (kStage == 2) {
+    if (lane == 0) {
+      mbar_init(wbar, 1u);
+      mbar_init(wbar + 1, 1u);
+    }
+    fence_mbar_init();
+    __syncwarp();
+    if (lane == 0 && gfirst < a.n_groups) issue(gfirst, 0u);
+  }
+  uint32_t it = 0;
+  for (uint32_t gi = gfirst; gi < a.n_groups; gi += nw, it++) {
     const long long t0 = clock64();
     const DecodeGroup gd = a.groups[gi];
+    const uint32_t b = it & 1u;
+    WS src;
+    if (kStage == 1) {
+      if (lane == 0 && gi + nw < a.n_groups) {
+        const DecodeGroup dn = a.groups[gi + nw];
+        const uint64_t hi = min(dn.w0 + dn.wn, a.wend);
+        if (hi > dn.w0) prefetch_l2(g.words + dn.w0, (hi - dn.w0) * 4);
+      }
+    }
+    if constexpr (kStage == 2) {
+      // the other buffer's last reader (the previous group) is done: it
+      // receives the next group's span while this one is decoded
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0 && gi + nw < a.n_groups) issue(gi + nw, b ^ 1u);
+      if (!__all_sync(kFull, mbar_wait(wbar + b, phase[b], kBulkWaitTries))) {
+        if (lane == 0) set_error(a.err, kErrTimeout);
+        // neither copy may still write the buffers when the warp leaves
+        mbar_wait(wbar + b, phase[b], kBulkWaitTries);
+        if (gi + nw < a.n_groups) mbar_wait(wbar + (b ^ 1u), phase[b ^ 1u], kBulkWaitTries);
+        break;
+      }
+      phase[b] ^= 1u;
+      uint64_t lo;
+      uint32_t n;
+      span_of(gd, lo, n);
+      src = StagedWords{g.words, wspan + b * kSpanWords, lo, n};
+    } else {
+      src = GWords{g.words};
+    }
     const uint32_t pk = gd.p0 + lane;
     uint4 ix = make_uint4(0u, 0u, 0u, 0u);
     if (pk < g.n_c) ix = a.pidx[pk];
@@ -1121,7 +1195,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
     bool bad = false;
     uint32_t cnt = 0, items = 0, node = 0;
     uint64_t q = 0, end = 0;
-    BitReader r;
+    BitReaderT<WS> r;
     if (act) {
       const uint64_t o0 = g.offsets[p];
       end = g.offsets[p + 1];
@@ -1130,7 +1204,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
       if (q >= end) {
         bad = true;
       } else {
-        r.seek(g.words, q);
+        r.seek(src, q);
         cnt = r.gamma(bad);
         if (!itv) {
           items = cnt;
@@ -1248,7 +1322,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
     if (__any_sync(kFull, coop)) {
       uint32_t left_todo = 0, nextbase = 0, w = 0;
       if (coop) {
-        r.seek(g.words, q);
+        r.seek(src, q);
         left_todo = r.gamma(bad);
       }
       // a section's last segment takes the overflow of the one before: < 512 bits, < 256 pairs
@@ -1306,9 +1380,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   busy_mark(a, 0, true);
 }
 
-template __global__ void k_decode_two_pass<0>(IterArgs a);
-template __global__ void k_decode_two_pass<1>(IterArgs a);
-template __global__ void k_decode_two_pass<2>(IterArgs a);
+#define LPA_DECODE_FORMS(G)                                  \
+  template __global__ void k_decode_two_pass<G, 0>(IterArgs a); \
+  template __global__ void k_decode_two_pass<G, 1>(IterArgs a); \
+  template __global__ void k_decode_two_pass<G, 2>(IterArgs a);
+LPA_DECODE_FORMS(0)
+LPA_DECODE_FORMS(1)
+LPA_DECODE_FORMS(2)
+#undef LPA_DECODE_FORMS
 
 namespace {
 
@@ -1701,10 +1780,27 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
 template __global__ void k_count_two_pass<false>(IterArgs a);
 template __global__ void k_count_two_pass<true>(IterArgs a);
 
-void launch_decode_two_pass(uint32_t gather_cache, int grid, cudaStream_t s, const IterArgs &a) {
-  if (gather_cache == 1) k_decode_two_pass<1><<<grid, kThreads, 0, s>>>(a);
-  else if (gather_cache == 2) k_decode_two_pass<2><<<grid, kThreads, 0, s>>>(a);
-  else k_decode_two_pass<0><<<grid, kThreads, 0, s>>>(a);
+template <int G>
+static void launch_decode_form(uint32_t stage, int grid, cudaStream_t s, const IterArgs &a) {
+  if (stage == 1) k_decode_two_pass<G, 1><<<grid, kThreads, 0, s>>>(a);
+  else if (stage == 2) k_decode_two_pass<G, 2><<<grid, kThreads, kSpanSmemBytes, s>>>(a);
+  else k_decode_two_pass<G, 0><<<grid, kThreads, 0, s>>>(a);
+}
+
+cudaError_t prepare_decode_two_pass() {
+  cudaError_t e = cudaFuncSetAttribute(k_decode_two_pass<0, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(kSpanSmemBytes));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_decode_two_pass<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSpanSmemBytes));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_decode_two_pass<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSpanSmemBytes));
+  return e;
+}
+
+void launch_decode_two_pass(uint32_t gather_cache, uint32_t stage, int grid, cudaStream_t s, const IterArgs &a) {
+  if (gather_cache == 1) launch_decode_form<1>(stage, grid, s, a);
+  else if (gather_cache == 2) launch_decode_form<2>(stage, grid, s, a);
+  else launch_decode_form<0>(stage, grid, s, a);
 }
 
 void launch_count_two_pass(bool bulk, int grid, cudaStream_t s, const IterArgs &a) {
@@ -1713,10 +1809,12 @@ void launch_count_two_pass(bool bulk, int grid, cudaStream_t s, const IterArgs &
 }
 
 cudaError_t occupancy_decode_two_pass(int *blocks) {
+  // the forms without shared-memory staging (the default); the staged form
+  // holds more shared memory and runs fewer blocks per SM
   int b0 = 1, b1 = 1, b2 = 1;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_decode_two_pass<0>, kThreads, 0);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_decode_two_pass<1>, kThreads, 0);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_decode_two_pass<2>, kThreads, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_decode_two_pass<0, 0>, kThreads, 0);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_decode_two_pass<1, 0>, kThreads, 0);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_decode_two_pass<2, 0>, kThreads, 0);
   *blocks = b0 < b1 ? (b0 < b2 ? b0 : b2) : (b1 < b2 ? b1 : b2);
   return e;
 }

@@ -48,8 +48,14 @@ struct WorkItem {
 // plan segment its cycles are booked to.
 struct DecodeGroup {
   uint32_t p0, j0, nlanes, seg;
+  uint64_t w0;      // the stream words its segments read: [w0, w0 + wn)
+  uint32_t wn, pad;
 };
 constexpr uint32_t kDecodeWindow = 768;  // staged ids per warp of the pre-pass
+// lpa_tune.stage_stream 2: words of a group's stream span one shared-memory
+// buffer holds (32 segments of < 512 bits plus their headers fit)
+constexpr uint32_t kSpanWords = 576;
+constexpr uint32_t kSpanSmemBytes = kWarps * 2 * kSpanWords * 4;  // its two buffers per warp (dynamic)
 
 // Work of the two-pass count pass (k_count_two_pass): positions p0 ..
 // p0 + np - 1, all of one kind, whose labels the pre-pass wrote to the
@@ -141,6 +147,9 @@ struct IterArgs {
   // ids [gbase[k], gbase[k + 1]); n_gbase = 0: one graph
   const uint32_t *gbase;
   uint32_t n_gbase;
+  // stream words [0, wend) that bulk copies may read (a multiple of 4: the
+  // copies move whole 16-byte units inside the stream's allocation)
+  uint64_t wend;
 };
 
 // The id base of the graph that owns vertex `node`.  The sketch hashes a
@@ -196,7 +205,7 @@ __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs);
 
 __global__ void k_iterate(IterArgs a);
 // kGather: the cache path of the residual label reads (lpa_tune.gather_cache)
-template <int kGather>
+template <int kGather, int kStage>
 __global__ void k_decode_two_pass(IterArgs a);
 // V2 for tiny vertices: a lane per vertex.
 __global__ void k_packed(IterArgs a);
@@ -207,10 +216,12 @@ __global__ void k_count_two_pass(IterArgs a);
 
 // The template forms of the two-pass kernels are launched and sized only in
 // the file that defines them (lp_kernels.cu):
-// k_decode_two_pass<gather_cache> on `grid` blocks of kThreads;
-void launch_decode_two_pass(uint32_t gather_cache, int grid, cudaStream_t s, const IterArgs &a);
+// k_decode_two_pass<gather_cache, stage_stream> on `grid` blocks of kThreads;
+void launch_decode_two_pass(uint32_t gather_cache, uint32_t stage, int grid, cudaStream_t s, const IterArgs &a);
 // k_count_two_pass<bulk> on `grid` blocks of kThreads with kCountSmemBytes;
 void launch_count_two_pass(bool bulk, int grid, cudaStream_t s, const IterArgs &a);
+// allows the stage_stream 2 forms their dynamic shared memory (once per device)
+cudaError_t prepare_decode_two_pass();
 // the fewest resident blocks per SM over each kernel's forms.
 cudaError_t occupancy_decode_two_pass(int *blocks);
 cudaError_t occupancy_count_two_pass(int *blocks);

@@ -169,16 +169,26 @@ __device__ void plan_segment(const PlanArgs &a, uint32_t i) {
   if (tp && si.region == 0) {
     // decode groups: 32 consecutive 256-bit segments of the positions,
     // spanning at most 32 positions
+    // first bit of segment j of position q (interval segments first)
+    const auto seg_bit = [&](uint32_t q, uint32_t jq, const uint4 &ix) {
+      return a.offsets[q] + (jq < ix.z ? uint64_t(ix.x) + uint64_t(kSegBits) * jq
+                                       : uint64_t(ix.y) + uint64_t(kSegBits) * (jq - ix.z));
+    };
     uint32_t p = si.begin, j = 0;
     while (p < si.end) {
-      DecodeGroup gd{p, j, 0u, s};
-      uint32_t positions = 0;
+      DecodeGroup gd{p, j, 0u, s, 0ull, 0u, 0u};
+      const uint64_t first = seg_bit(p, j, a.pidx[p]);
+      uint32_t positions = 0, lp = p, lj = j;
       while (p < si.end && gd.nlanes < 32 && positions < 32) {
         const uint4 ix = a.pidx[p];
         const uint32_t ns = ix.z + ix.w;
         const uint32_t take = min(ns - j, 32u - gd.nlanes);
         gd.nlanes += take;
         positions++;
+        if (take) {
+          lp = p;
+          lj = j + take - 1;
+        }
         if (j + take == ns) {
           p++;
           j = 0;
@@ -186,6 +196,13 @@ __device__ void plan_segment(const PlanArgs &a, uint32_t i) {
           j += take;
         }
       }
+      // the span its lanes read: from the first segment to the end of the
+      // last (a section's last segment is under 512 bits), plus the 2 words
+      // a reader loads ahead
+      const uint64_t last_end = min(a.offsets[lp + 1], seg_bit(lp, lj, a.pidx[lp]) + 2 * kSegBits);
+      gd.w0 = first >> 5;
+      const uint64_t wn = (last_end >> 5) + 3 - gd.w0;
+      gd.wn = uint32_t(wn < 0xFFFFFFFFull ? wn : 0xFFFFFFFFull);
       if (gd.nlanes) {
         if (kEmit) a.groups[o[kLGroups] + c[kLGroups]] = gd;
         c[kLGroups]++;

@@ -614,6 +614,7 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.gtab_slots = h->gtab_slots;
   a.gbase = h->d_gbase;
   a.n_gbase = h->d_gbase ? h->n_graphs : 0u;
+  a.wend = (h->nwords + 4) & ~uint64_t(3);
   return a;
 }
 
@@ -639,7 +640,7 @@ static void enqueue_iteration(lpa_handle *h, unsigned long long *changed, uint32
   };
   mark(-1);
   if (h->n_groups) {
-    launch_decode_two_pass(h->tune.gather_cache, h->grid_decode, h->stream, a);
+    launch_decode_two_pass(h->tune.gather_cache, h->tune.stage_stream, h->grid_decode, h->stream, a);
     h->launches++;
     mark(0);
   }
@@ -714,8 +715,9 @@ static void enqueue_streamed_iteration(lpa_handle *h, unsigned long long *change
     a.packed = r.packed;
     a.n_packed = r.n_packed;
     a.scratch = h->d_scratch ? scratch_base(h, r.a0) : nullptr;
+    a.wend = r.w1 & ~uint64_t(3);
     if (r.n_groups) {
-      launch_decode_two_pass(h->tune.gather_cache, r.grid_decode, h->stream, a);
+      launch_decode_two_pass(h->tune.gather_cache, h->tune.stage_stream, r.grid_decode, h->stream, a);
       h->launches++;
     }
     if (r.n_cblock + r.n_cwarp) {
@@ -845,6 +847,7 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     }
     check(h, cudaFuncSetAttribute(k_iterate, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes)),
           "smem attr");
+    check(h, prepare_decode_two_pass(), "smem attr");
     check(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ, k_iterate, kThreads, kSmemBytes), "occupancy");
     h->occ = std::max(1, h->occ);
     h->grid = h->num_sms * h->occ;
@@ -1204,7 +1207,7 @@ lpa_status lpa_set_dispatch(lpa_handle *h, int dispatch, int force_variant) {
 static bool tune_valid(const lpa_tune &t) {
   return t.group_positions >= 1 && t.group_positions <= 32 && t.warp_positions >= 1 && t.warp_positions <= 32 &&
          t.warp_max_degree >= 32 && t.warp_max_degree <= kCountWarpMax && t.warp_claim >= 1 && t.warp_claim <= 8 &&
-         t.bulk_stage <= 1 && t.gather_cache <= 2;
+         t.bulk_stage <= 1 && t.gather_cache <= 2 && t.stage_stream <= 2;
 }
 
 // One iteration from the current labels, repeated; the labels are left as
@@ -1252,7 +1255,7 @@ static std::string tune_key(const lpa_handle *h) {
   uint64_t arcs = 0;
   for (const auto &sg : h->segs) arcs += sg.arcs;
   char buf[512];
-  std::snprintf(buf, sizeof(buf), "v4|%s|sm%d|n%llu|nc%llu|arcs%llu|cms%u|plan%016llx", gpu.c_str(), pr.multiProcessorCount,
+  std::snprintf(buf, sizeof(buf), "v5|%s|sm%d|n%llu|nc%llu|arcs%llu|cms%u|plan%016llx", gpu.c_str(), pr.multiProcessorCount,
                 (unsigned long long)h->n, (unsigned long long)h->n_c, (unsigned long long)arcs,
                 h->opts.cms_threshold, (unsigned long long)fnv);
   return buf;
@@ -1291,7 +1294,7 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
         std::string k;
         lpa_tune t{};
         if (ls >> k >> t.group_positions >> t.warp_positions >> t.warp_max_degree >> t.warp_claim >> t.bulk_stage >>
-                t.gather_cache &&
+                t.gather_cache >> t.stage_stream &&
             k == key && tune_valid(t)) {
           h->tune = t;
           found = true;
@@ -1308,9 +1311,9 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
       static const uint32_t groups[] = {8, 16, 24, 32}, warps[] = {1, 2, 4, 8, 16},
                             degs[] = {63, 127, 255, kCountWarpMax}, claims[] = {1, 2, 4, 8}, flags[] = {0, 1, 2};
       for (int sweep = 0; sweep < 2; sweep++) {
-        for (int knob = 0; knob < 6; knob++) {
+        for (int knob = 0; knob < 7; knob++) {
           const uint32_t *vals = knob == 0 ? groups : knob == 1 ? warps : knob == 2 ? degs : knob == 3 ? claims : flags;
-          const int nv = knob == 1 ? 5 : knob == 4 ? 2 : knob == 5 ? 3 : 4;
+          const int nv = knob == 1 ? 5 : knob == 4 ? 2 : knob >= 5 ? 3 : 4;
           for (int i = 0; i < nv; i++) {
             lpa_tune cand = best;
             uint32_t &slot = knob == 0 ? cand.group_positions
@@ -1318,7 +1321,8 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
                              : knob == 2 ? cand.warp_max_degree
                              : knob == 3 ? cand.warp_claim
                              : knob == 4 ? cand.bulk_stage
-                                         : cand.gather_cache;
+                             : knob == 5 ? cand.gather_cache
+                                         : cand.stage_stream;
             if (slot == vals[i]) continue;
             slot = vals[i];
             h->tune = cand;
@@ -1337,7 +1341,8 @@ lpa_status lpa_autotune(lpa_handle *h, const char *cache_path, int repeats, lpa_
       if (cache_path) {
         std::ofstream o(cache_path, std::ios::app);
         o << key << ' ' << best.group_positions << ' ' << best.warp_positions << ' ' << best.warp_max_degree << ' '
-          << best.warp_claim << ' ' << best.bulk_stage << ' ' << best.gather_cache << ' ' << best_ms << '\n';
+          << best.warp_claim << ' ' << best.bulk_stage << ' ' << best.gather_cache << ' ' << best.stage_stream << ' '
+          << best_ms << '\n';
       }
     }
     if (out) *out = h->tune;

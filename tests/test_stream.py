@@ -83,3 +83,16 @@ def test_vertex_beyond_the_budget_is_refused():
     with pytest.raises(L.LpaError) as e:
         L.Propagator(g, stream_budget=64 << 10)
     assert e.value.status == L.Status.CAPACITY
+
+
+@pytest.mark.parametrize("stage", [1, 2])
+def test_streamed_two_pass_with_staged_stream_spans(stage):
+    """The pre-pass's stream staging (L2 prefetch, or bulk copies into shared
+    memory) reading from a streamed range's buffer: same labels."""
+    g = L.HostGraph.rmat(16, 16, seed=1).compress(32, 128)
+    arr = g.arrays()
+    opts = dict(cms_threshold=64, stream_budget=2 << 20, dispatch=L.Dispatch.FORCE,
+                force_variant=int(L.Variant.TWO_PASS))
+    with L.Propagator(g, **opts) as p:
+        p.set_tune(32, 4, 511, 2, 1, 0, stage)
+        _check(p, arr, 64, 5)

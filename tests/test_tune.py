@@ -21,12 +21,16 @@ def _two_pass(p):
     p.set_plan(plan)
 
 
-@pytest.mark.parametrize("knobs", [(1, 1, 32, 1, 0, 0), (7, 3, 100, 8, 1, 1), (32, 32, 511, 5, 0, 2),
-                                   (32, 4, 511, 2, 1, 0)])
-def test_knobs_keep_labels_exact(knobs):
+@pytest.mark.parametrize("knobs", [(1, 1, 32, 1, 0, 0, 0), (7, 3, 100, 8, 1, 1, 1), (32, 32, 511, 5, 0, 2, 2),
+                                   (32, 4, 511, 2, 1, 0, 2), (32, 4, 511, 2, 0, 1, 2), (16, 8, 255, 2, 0, 0, 1)])
+@pytest.mark.parametrize("case", ["rmat_t16", "stress", "copy_t16"])
+def test_knobs_keep_labels_exact(knobs, case):
     """bulk_stage = 1 stages the several-vertices items by bulk copies;
-    gather_cache picks the pre-pass's label read path (hot ids / L2 / L1)."""
-    g, ref = _load("rmat_t16")
+    gather_cache picks the pre-pass's label read path (hot ids / L2 / L1);
+    stage_stream moves each decode group's stream span ahead of its decode
+    (1 a bulk prefetch into L2, 2 double-buffered bulk copies into shared
+    memory); the stress graph has long intervals and many segments per vertex."""
+    g, ref = _load(case)
     hist, changed = oracle.lp_run(ref["row"], ref["clm"], 4, 64)
     with L.Propagator(g, cms_threshold=64) as p:
         _two_pass(p)
@@ -42,7 +46,7 @@ def test_out_of_range_knobs_are_refused():
     with L.Propagator(g) as p:
         before = p.get_tune().as_tuple()
         for bad in [(0, 4, 511, 2), (33, 4, 511, 2), (32, 4, 31, 2), (32, 4, 512, 2), (32, 4, 511, 9),
-                    (32, 4, 511, 2, 2), (32, 4, 511, 2, 0, 3)]:
+                    (32, 4, 511, 2, 2), (32, 4, 511, 2, 0, 3), (32, 4, 511, 2, 0, 0, 3)]:
             with pytest.raises(L.LpaError) as e:
                 p.set_tune(*bad)
             assert e.value.status == L.Status.INVALID_ARG
