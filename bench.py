@@ -52,9 +52,12 @@ WORKLOADS = {
     # [1k, 256k], even graphs road grids (p=0.7), odd graphs R-MAT (edge factor 8),
     # threshold 16, per-graph early exit (the 4096-graph [1k, 2M] batch scaled down)
     "batch-256": dict(kind="batch", graphs=256, n_lo=1000, n_hi=262144, seed=1, small_thresh=16, cms=0, iters=30),
-    # all 4096 graphs, sizes log-uniform in [1k, 128k] (the [1k, 2M] range would hold ~8e9 arcs)
+    # all 4096 graphs, sizes log-uniform in [1k, 128k]
     "batch-4096": dict(kind="batch", graphs=4096, n_lo=1000, n_hi=131072, seed=1, small_thresh=16, cms=0,
                        iters=30),
+    # the full batch: 4096 graphs, sizes log-uniform in [1k, 2M] (about 1.1e9 vertices, 1e10 arcs)
+    "batch-4096-full": dict(kind="batch", graphs=4096, n_lo=1000, n_hi=2_000_000, seed=1, small_thresh=16, cms=0,
+                            iters=30),
 }
 
 
@@ -101,28 +104,58 @@ def build_graph(w: dict):
 
 
 def build_batch(w: dict):
-    """The batched workload's graphs (seeded; seed + i for graph i)."""
+    """The batched workload's graphs (seeded; seed + i for graph i), generated
+    and compressed on all host cores (the generators release the GIL)."""
+    import concurrent.futures as cf
+
     import lpa_b200 as L
 
     rng = np.random.default_rng(w["seed"])
-    graphs = []
-    for i in range(w["graphs"]):
-        n = int(np.exp(rng.uniform(np.log(w["n_lo"]), np.log(w["n_hi"]))))
+    sizes = [int(np.exp(rng.uniform(np.log(w["n_lo"]), np.log(w["n_hi"])))) for _ in range(w["graphs"])]
+
+    def make(i):
+        n = sizes[i]
         if i % 2 == 0:
             side = max(4, int(round(np.sqrt(n))))
             g = L.HostGraph.road(side, side, seed=w["seed"] + i)
         else:
             g = L.HostGraph.rmat(max(8, int(np.ceil(np.log2(n)))), 8.0, seed=w["seed"] + i, n_limit=n)
-        g.compress(w["small_thresh"], 128)
-        graphs.append(g)
-    return graphs
+        g.compress(w["small_thresh"], 128, threads=1)
+        return g
+
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        return list(ex.map(make, range(w["graphs"])))
 
 
-def algorithmic_bytes(arr: dict) -> int:
+def verify_batch(bt, graphs, iters, max_check: int = 8) -> dict:
+    """Per-graph labels of the batch's last run against the oracle run alone
+    on that graph (same iterations, early exit), on a sample: the smallest and
+    the largest graph of each kind and graphs spread between them."""
+    import oracle
+
+    order = sorted(range(len(graphs)), key=lambda i: int(graphs[i].desc().num_vertices))
+    pick = sorted(set(order[:: max(1, len(order) // (max_check - 2))][: max_check - 2] + order[-2:]))
+    bad = 0
+    for i in pick:
+        row, clm = graphs[i].csr()
+        hist, _ = oracle.lp_run(row, clm, 30, early_exit=True)
+        want = hist[min(int(iters[i]), len(hist)) - 1] if len(hist) else np.arange(len(row) - 1, dtype=np.uint32)
+        bad += int(len(hist) != int(iters[i])) + int(np.count_nonzero(bt.labels(i) != want))
+    return {"graphs_checked": len(pick), "mismatches": bad,
+            "vertices_checked": int(sum(int(graphs[i].desc().num_vertices) for i in pick))}
+
+
+def graph_meta(g) -> dict:
+    """Sizes of a compressed host graph, read without copying its arrays."""
+    d = g.desc()
+    n, n_c = int(d.num_vertices), int(d.num_compressed)
+    return {"n": n, "n_c": n_c, "bits": int(d.offsets[n_c]) if n_c else 0, "m_small": int(d.num_small_arcs)}
+
+
+def algorithmic_bytes(meta: dict) -> int:
     """One iteration's compulsory bytes of one graph (see lpa_info)."""
-    n, n_c = arr["n"], arr["n_c"]
-    return ((int(arr["offsets"][-1]) + 7) // 8 + 8 * (n_c + 1) + 4 * n_c + 4 * (n - n_c + 1)
-            + 4 * len(arr["small_graph"]) + 12 * n)
+    n, n_c = meta["n"], meta["n_c"]
+    return ((meta["bits"] + 7) // 8 + 8 * (n_c + 1) + 4 * n_c + 4 * (n - n_c + 1) + 4 * meta["m_small"] + 12 * n)
 
 
 def run_batch(args, w, rank, world, local):
@@ -134,18 +167,14 @@ def run_batch(args, w, rank, world, local):
 
     device = f"cuda:{local}"
     graphs = build_batch(w)
-    arrs = [g.arrays() for g in graphs]
-    arcs = [int(len(a["small_graph"])) for a in arrs]
+    arrs = [graph_meta(g) for g in graphs]
     stream = torch.cuda.Stream(device=device)
     mode = L.BatchMode.LOCKSTEP if args.batch_mode == "lockstep" else L.BatchMode.QUEUE
     dispatch = L.Dispatch.LEARNED if args.dispatch == "learned" else L.Dispatch.FIXED
     with L.Batch(graphs, device=local, cms_threshold=w["cms"], stream=stream.cuda_stream, batch_mode=mode,
                  dispatch=dispatch) as bt:
         h = bt.handle()  # lockstep: the concatenated graph's handle
-        degs = []
-        for g in graphs:  # arcs per graph from the host CSR
-            row, _ = g.csr()
-            degs.append(int(row[-1]))
+        degs = [g.num_arcs() for g in graphs]  # arcs per graph from the host CSR
         for _ in range(args.warmup):
             iters = bt.run(w["iters"], early_exit=True)
         tune = None
@@ -176,7 +205,11 @@ def run_batch(args, w, rank, world, local):
         total_ms = max_over_ranks(total_ms, world, device)
         value = work * world / (total_ms / 1e3)
         # end to end: a run plus every graph's labels back to pinned host memory
-        outs = [torch.empty(a["n"], dtype=torch.int32, pin_memory=True) for a in arrs]
+        pinned = torch.empty(sum(a["n"] for a in arrs), dtype=torch.int32, pin_memory=True)
+        outs, at = [], 0
+        for a in arrs:
+            outs.append(pinned.narrow(0, at, a["n"]))
+            at += a["n"]
         lib = L.lib()
         import ctypes as C
 
@@ -188,6 +221,7 @@ def run_batch(args, w, rank, world, local):
                                                 arrs[gi]["n"]) == 0
         e2e_s = max_over_ranks(time.perf_counter() - e0, world, device)
         e2e_work = sum(int(d) * int(k) for d, k in zip(degs, it_e)) * max(1, args.e2e_steps)
+        verify = verify_batch(bt, graphs, it_e) if (rank == 0 and not args.no_cpu_baseline) else None
     peak, peak_kind = measured_peak_gbs()
     achieved = bytes_done / (total_ms / 1e3) / 1e9
     if rank == 0:
@@ -203,6 +237,7 @@ def run_batch(args, w, rank, world, local):
                              "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": peak_kind, "traffic": None},
                 "cpu_baseline": None,
+                "verify": verify,
                 "e2e": {"value": e2e_work * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": int(4 * sum(a["n"] for a in arrs))},
                 "gpu_launches": int(launches), "clocks": clk, "wall_s_timed": wall}

@@ -331,6 +331,14 @@ class HostGraph:
         r = _view(row, n.value + 1, np.uint64)
         return r, _view(clm, int(r[-1]) if len(r) else 0, np.uint32)
 
+    def num_arcs(self) -> int:
+        """Stored arcs of the CSR (no copy)."""
+        n = C.c_uint64()
+        row = C.POINTER(C.c_uint64)()
+        clm = C.POINTER(C.c_uint32)()
+        _check(lib().lpa_hg_csr(self._h, C.byref(n), C.byref(row), C.byref(clm)), "csr")
+        return int(row[n.value])
+
     def desc(self) -> GraphDesc:
         d = GraphDesc()
         _check(lib().lpa_hg_desc(self._h, C.byref(d)), "desc")

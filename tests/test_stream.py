@@ -77,8 +77,9 @@ def test_streamed_decode_matches_resident():
 
 
 def test_vertex_beyond_the_budget_is_refused():
-    """One hub's labels (degree 9674: 39 KB) cannot fit a 64 KB budget's
-    16 KB scratch: LPA_ERR_CAPACITY at create, not a fault."""
+    """One hub (degree 9674: about 18 KB of stream, 39 KB of labels) fits
+    neither a 64 KB budget's 16 KB stream buffers nor its 32 KB scratch:
+    LPA_ERR_CAPACITY at create, not a fault."""
     g = L.HostGraph.rmat(16, 16, seed=1).compress(32, 128)
     with pytest.raises(L.LpaError) as e:
         L.Propagator(g, stream_budget=64 << 10)
