@@ -83,6 +83,7 @@ struct BlockSh {
   uint64_t red[kWarps];
   uint64_t ibase, rbase, last_end;
   uint32_t nseg_i, nseg_r, item, items, bad;
+  uint32_t spill_n;  // labels a hub has written to its spill area so far
   uint32_t hepoch;  // epoch of the block's exact table
 };
 
@@ -142,6 +143,28 @@ struct CmsAddSink {
   }
 };
 
+// Passes every label on to `inner` and also writes it to spill[0..cap), one
+// reservation per 32 labels (warp-synchronous, like every sink): the sketch's
+// second pass over a decoded hub then reads the labels back instead of
+// decoding the hub again.
+template <class Sink>
+struct SpillSink {
+  Sink inner;
+  uint32_t *spill;
+  uint32_t cap;
+  uint32_t *count;  // shared
+  __device__ __forceinline__ void operator()(bool ok, uint32_t lab) const {
+    inner(ok, lab);
+    const uint32_t m = __ballot_sync(kFull, ok);
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if (lane == 0 && m) base = atomicAdd(count, uint32_t(__popc(m)));
+    base = __shfl_sync(kFull, base, 0);
+    const uint32_t at = base + uint32_t(__popc(m & ((1u << lane) - 1u)));
+    if (ok && at < cap) spill[at] = lab;
+  }
+};
+
 // Second sketch pass: read-only, so every lane looks up its own label.
 struct CmsBestSink {
   const uint32_t *cms;
@@ -177,6 +200,25 @@ __device__ __forceinline__ void block_gather_from(uint32_t *stage, const uint32_
     for (int u = 0; u < 4; u++) {
       const uint32_t k = k0 + u * kThreads;
       if (k < total) stage[k] = v[u];
+    }
+  }
+}
+
+// Labels src[0..total) from global memory (a hub's spill area), 4 loads per
+// thread in flight, into sink; block-synchronous.
+template <class Sink>
+__device__ __forceinline__ void block_consume_global(const uint32_t *src, uint32_t total, const Sink &sink) {
+  for (uint32_t k0 = 0; k0 < total; k0 += 4 * kThreads) {
+    uint32_t v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t k = k0 + u * kThreads + threadIdx.x;
+      v[u] = k < total ? __ldcg(src + k) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t k = k0 + u * kThreads + threadIdx.x;
+      sink(k < total, v[u]);
     }
   }
 }
@@ -421,11 +463,23 @@ __device__ void heavy_vertex(const IterArgs &a, const Ctx &c, BlockSh &sh, uint3
     for (uint32_t i = t; i < kCmsDepth * kCmsWidth; i += kThreads) cms[i] = 0u;
     __syncthreads();
     const uint32_t lb = label_base(a, node);
-    const bool staged = heavy_produce(a, c, sh, stage, p, node, d, from_scratch, CmsAddSink{cms, a.seeds, lb});
+    // a hub decoded here keeps its labels in the block's spill area (when it
+    // fits), so the second pass reads them back instead of decoding again
+    const bool decoded = p < g.n_c && !from_scratch;
+    uint32_t *spill = (a.hub_spill && decoded && d <= a.hub_spill_words)
+                          ? a.hub_spill + uint64_t(blockIdx.x) * a.hub_spill_words
+                          : nullptr;
+    if (t == 0) sh.spill_n = 0;
+    __syncthreads();
+    const CmsAddSink s1{cms, a.seeds, lb};
+    const bool staged = spill ? heavy_produce(a, c, sh, stage, p, node, d, from_scratch,
+                                              SpillSink<CmsAddSink>{s1, spill, d, &sh.spill_n})
+                              : heavy_produce(a, c, sh, stage, p, node, d, from_scratch, s1);
     __syncthreads();
     CmsBestSink s2{cms, a.seeds, lb, &best};
     if (staged) heavy_consume_staged(sh, stage, s2);
     else if ((p >= g.n_c || from_scratch) && d <= kStage) block_consume_stage(stage, d, s2);
+    else if (spill && sh.spill_n == d) block_consume_global(spill, d, s2);
     else heavy_produce(a, c, sh, stage, p, node, d, from_scratch, s2);
     __syncthreads();
     // leave no counter behind that an epoch table could read as its own slot
@@ -865,7 +919,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
   flush_changed(c.changed, changed);
 }
 
-__device__ __forceinline__ uint32_t packed_vertex(const IterArgs &a, const Ctx &c, uint32_t p);
+__device__ __forceinline__ uint32_t packed_vertex(const IterArgs &a, const Ctx &c, uint32_t p, uint32_t *lab);
 
 // Many graphs, one persistent launch.  A ring queue holds (graph,
 // iteration, segment) items; iteration 0 of every graph is queued by the
@@ -957,7 +1011,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchArgs b) {
       block_segment(ia, c, sh, stage, tab, wstage, wslots, wepoch, s, sg, false, changed);
     } else if (v == kVarPackedLanes) {
       // a tiny segment: one thread per position (<= 256 positions)
-      if (sg.begin + t < sg.end) changed += packed_vertex(ia, c, sg.begin + t);
+      if (sg.begin + t < sg.end) changed += packed_vertex(ia, c, sg.begin + t, stage + t * kPackedMaxDeg);
     } else {
       const uint32_t p0 = sg.begin + warp * 32u;  // light segments hold at most 8 chunks
       if (p0 < sg.end) light_chunk(ia, c, wstage, wslots, wepoch, s, p0, min(sg.end, p0 + 32u), v, changed);
@@ -1010,12 +1064,14 @@ __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs) {
 // whole bit range (or its small-CSR list), gathering each label as soon as
 // its id is decoded, then takes the most frequent of its labels (smallest on
 // ties) by pairwise counts.  Returns 1 when the label changed.
-__device__ __forceinline__ uint32_t packed_vertex(const IterArgs &a, const Ctx &c, uint32_t p) {
+// lab: this thread's kPackedMaxDeg label slots (shared memory in k_packed,
+// where a lane's slots start kPackedMaxDeg words after the previous lane's:
+// an odd stride, so the 32 lanes' k-th slots fall in 32 different banks).
+__device__ __forceinline__ uint32_t packed_vertex(const IterArgs &a, const Ctx &c, uint32_t p, uint32_t *lab) {
   const DevGraph &g = a.g;
   const uint32_t node = g.vertices[p];
   const uint32_t d = g.deg[p];
   const uint32_t old = ld_label(c, node);
-  uint32_t lab[kPackedMaxDeg];
   uint32_t k = 0;
   bool bad = d > kPackedMaxDeg;
   if (!bad && p < g.n_c) {
@@ -1049,6 +1105,9 @@ __device__ __forceinline__ uint32_t packed_vertex(const IterArgs &a, const Ctx &
 // per position (packed_vertex), 32 vertices per warp.  No shared memory, no
 // warp-wide steps.
 __global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
+  // per thread kPackedMaxDeg label slots: a per-thread array indexed at run
+  // time would live in local memory
+  __shared__ uint32_t slab[kThreads * kPackedMaxDeg];
   const Ctx c = resolve(a);
   busy_mark(a, 3, false);
   const uint32_t lane = threadIdx.x & 31u;
@@ -1057,7 +1116,7 @@ __global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
   for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n_packed; i += nw) {
     const long long t0 = clock64();
     const PackedChunk ch = a.packed[i];
-    const uint32_t mine = lane < ch.np ? packed_vertex(a, c, ch.p0 + lane) : 0u;
+    const uint32_t mine = lane < ch.np ? packed_vertex(a, c, ch.p0 + lane, slab + threadIdx.x * kPackedMaxDeg) : 0u;
     changed += mine;
     const uint32_t sc = __reduce_add_sync(kFull, mine);
     if (lane == 0) {

@@ -150,6 +150,10 @@ struct IterArgs {
   // stream words [0, wend) that bulk copies may read (a multiple of 4: the
   // copies move whole 16-byte units inside the stream's allocation)
   uint64_t wend;
+  // per block of k_iterate: hub_spill_words labels of the sketch hub it is
+  // decoding (nullptr: none; a hub decodes twice)
+  uint32_t *hub_spill;
+  uint32_t hub_spill_words;
 };
 
 // The id base of the graph that owns vertex `node`.  The sketch hashes a

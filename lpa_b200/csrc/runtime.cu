@@ -223,6 +223,16 @@ static void build_segments(lpa_handle *h) {
 // few launches and one copy of the list sizes, not a host loop over n.
 static void upload_range_lists(lpa_handle *h);
 
+// The block path's sketch hubs keep their labels between the sketch's two
+// passes in a per-block spill area (at most 2 GiB in all; larger hubs decode
+// twice), allocated once a plan gives k_iterate heavy items.
+static void ensure_hub_spill(lpa_handle *h) {
+  if (h->d_hub_spill || h->n_heavy == 0 || h->max_sketch_deg == 0) return;
+  const uint64_t per_block = std::min<uint64_t>(h->max_sketch_deg, (2ull << 30) / 4 / uint64_t(std::max(1, h->grid)));
+  h->d_hub_spill = dalloc<uint32_t>(h, per_block * uint64_t(h->grid), "hub spill");
+  h->hub_spill_words = uint32_t(per_block);
+}
+
 static void upload_lists(lpa_handle *h) {
   h2d(h, h->d_seg_var, h->variant.data(), h->variant.size(), "upload variants");
   if (h->streamed) {
@@ -288,6 +298,7 @@ static void upload_lists(lpa_handle *h) {
   h->n_groups = out.n_groups;
   h->n_cblock = out.n_cblock;
   h->n_cwarp = out.n_cwarp;
+  ensure_hub_spill(h);
   h->plan_version++;
   // one warp per decode group, kThreads / 32 warps per block
   h->grid_decode = int(std::max<uint64_t>(
@@ -368,6 +379,7 @@ static void upload_range_lists(lpa_handle *h) {
     h->n_cblock += r.n_cblock;
     h->n_cwarp += r.n_cwarp;
   }
+  ensure_hub_spill(h);
   h->plan_version++;
 }
 
@@ -557,6 +569,7 @@ static void build_plan(lpa_handle *h) {
     const uint32_t d = h->h_deg[p];
     const bool cms = h->opts.cms_threshold != 0 && d >= h->opts.cms_threshold;
     if (!cms && d > kBlockMaxSmemDeg) big = std::max<uint64_t>(big, d);
+    if (cms) h->max_sketch_deg = std::max(h->max_sketch_deg, d);
   }
   if (big) {
     h->gtab_slots = next_pow2_host(2 * big);
@@ -615,6 +628,8 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.gbase = h->d_gbase;
   a.n_gbase = h->d_gbase ? h->n_graphs : 0u;
   a.wend = (h->nwords + 4) & ~uint64_t(3);
+  a.hub_spill = h->d_hub_spill;
+  a.hub_spill_words = h->hub_spill_words;
   return a;
 }
 

@@ -129,6 +129,9 @@ struct lpa_handle {
   uint64_t *d_arc_off = nullptr;
   uint32_t *d_scratch = nullptr;
   uint32_t *d_gtab = nullptr;
+  uint32_t *d_hub_spill = nullptr;  // per block of k_iterate: a sketch hub's labels (second pass)
+  uint32_t hub_spill_words = 0;
+  uint32_t max_sketch_deg = 0;      // largest degree at or above the sketch threshold
   uint32_t gtab_slots = 0;
   int gtab_blocks = 0;
   long long *d_seg_cycles = nullptr;
