@@ -116,3 +116,26 @@ def test_road_generator_shape():
     src = np.repeat(np.arange(n), deg.astype(np.int64))
     fwd = set(zip(src.tolist(), clm.tolist()))
     assert all((v, u) in fwd for (u, v) in list(fwd)[:5000])
+
+
+@pytest.mark.skipif(not oracle.REF_BIN.exists(), reason="the reference compressor was not built here")
+def test_encoder_matches_reference_on_the_benchmark_family(tmp_path):
+    """The benchmark's graph family at a size the reference compressor handles
+    in seconds: R-MAT scale 18, edge factor 16, symmetrised, BFS order,
+    threshold 32 (7.6M arcs, hubs with intervals).  The reference's own
+    CgrCompressor (built from its sources into oracle/_ref) and this library
+    write byte-identical files from the same edge list (which, like the
+    reference's ingest, ends at the largest id that has an edge)."""
+    import subprocess
+
+    el = str(tmp_path / "e.txt")
+    L.HostGraph.rmat(18, 16.0, seed=1).write_edge_list(el, False)
+    subprocess.run([str(oracle.REF_BIN), el, "1", "32"], check=True, capture_output=True)
+    g = L.HostGraph.read_edge_list(el, True)
+    g.compress(32, 128)
+    out = str(tmp_path / "ours")
+    g.write_cgr(out)
+    for ext in EXTS:
+        assert os.path.exists(el + ext) == os.path.exists(out + ext), ext
+        if os.path.exists(el + ext):
+            assert filecmp.cmp(el + ext, out + ext, shallow=False), ext
