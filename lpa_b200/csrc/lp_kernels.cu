@@ -968,6 +968,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchArgs b) {
     const uint32_t gi = uint32_t(e >> 44), it = uint32_t(e >> 32) & 0xFFFu, s = uint32_t(e);
     if (t == 0) {
       const BatchGraph &bg = b.graphs[gi];
+      ia = IterArgs{};  // every field this launch does not use is zero (null): no hub spill, no scratch
       ia.g = bg.g;
       ia.labs0 = bg.labs0;
       ia.labs1 = bg.labs1;
