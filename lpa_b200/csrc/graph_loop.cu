@@ -123,7 +123,7 @@ lpa_status lpa_run_graph(lpa_handle *h, int max_iter, bool early_exit, int *iter
   ctl[2] = early_exit ? 1u : 0u;
   e = cudaMemsetAsync(h->d_changed, 0, size_t(max_iter + 2) * sizeof(unsigned long long), h->stream);
   if (e != cudaSuccess) return fail(e, "clear counters");
-  e = cudaMemsetAsync(h->d_work, 0, size_t(4 * (max_iter + 2)) * sizeof(uint32_t), h->stream);
+  e = cudaMemsetAsync(h->d_work, 0, size_t(lpa_dev::kWorkCounters) * size_t(max_iter + 2) * sizeof(uint32_t), h->stream);
   if (e != cudaSuccess) return fail(e, "clear work counters");
   e = cudaMemcpyAsync(h->d_loop_it, ctl, 3 * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream);
   if (e != cudaSuccess) return fail(e, "loop control");

@@ -855,7 +855,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_iterate(IterArgs a) {
   const Ctx c = resolve(a);
   busy_mark(a, 2, false);
   unsigned long long changed = 0;
-  uint32_t *qctr = a.work + 4 * (a.it_dev ? c.it : 0u);
+  uint32_t *qctr = a.work + kWorkCounters * (a.it_dev ? c.it : 0u) + kWqHeavy;
 
   // per-warp staging and exact table of the warp-scope paths
   unsigned long long *wslots = reinterpret_cast<unsigned long long *>(tab) + warp * kWarpSlots;
@@ -1134,7 +1134,8 @@ __global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
 // Two-pass variant, pass 1.  Every 256-bit segment of the two-pass positions
 // is decoded by one lane, which writes the labels of its ids (not the ids) to
 // the scratch, so pass 2 only counts.  A warp takes one decode group (32
-// segments).  Lane l finds its position with a warp scan of the positions'
+// segments) at a time from the iteration's work queue (IterArgs::work slot
+// kWqGroups, zeroed before the launch).  Lane l finds its position with a warp scan of the positions'
 // segment counts and a 5-step search; the lanes of one position reserve their
 // output range with one atomicAdd on the position's cursor, since the labels
 // of a position may sit in any order.  No block barriers: warps run alone.
@@ -1167,8 +1168,20 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   const uint32_t hot = uint32_t(g.n >> 6);  // kGather 0: ids below read through L1
   busy_mark(a, 0, false);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t gfirst = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  // Decode groups come from the iteration's work queue, kGroupClaim at a
+  // time, each warp's next claim made one ahead so that its atomic is off the
+  // critical path.  A fixed grid-stride assignment left SMs idle for 28 % of
+  // the kernel at R-MAT scale 22 (ncu: 0.66 ms of SM activity in a 0.92 ms
+  // launch): groups whose interval segments expand thousands of ids finished
+  // late on the warps that drew them.
+  uint32_t *gctr = a.work + kWorkCounters * (a.it_dev ? c.it : 0u) + kWqGroups;
+  const auto claim = [&]() {
+    uint32_t x = 0;
+    if (lane == 0) x = atomicAdd(gctr, kGroupClaim);
+    return __shfl_sync(kFull, x, 0);
+  };
+  uint32_t gi = claim();
+  uint32_t ahead = claim(), cend = gi + kGroupClaim;
   uint32_t *wspan = sspan + (kStage == 2 ? warp * 2 * kSpanWords : 0);
   uint64_t *wbar = sbar + (kStage == 2 ? warp * 2 : 0);
   uint32_t phase[2] = {0u, 0u};
@@ -1193,17 +1206,28 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
     }
     fence_mbar_init();
     __syncwarp();
-    if (lane == 0 && gfirst < a.n_groups) issue(gfirst, 0u);
+    if (lane == 0 && gi < a.n_groups) issue(gi, 0u);
   }
-  uint32_t it = 0;
-  for (uint32_t gi = gfirst; gi < a.n_groups; gi += nw, it++) {
+  // the group after gi: the next of its claim, else the first of the claim
+  // made ahead (which then becomes the current claim)
+  const auto advance = [&]() {
+    if (gi + 1u < cend) {
+      gi++;
+    } else {
+      gi = ahead;
+      cend = ahead + kGroupClaim;
+      ahead = claim();
+    }
+  };
+  for (uint32_t it = 0; gi < a.n_groups; it++, advance()) {
     const long long t0 = clock64();
     const DecodeGroup gd = a.groups[gi];
     const uint32_t b = it & 1u;
+    const uint32_t gnext = gi + 1u < cend ? gi + 1u : ahead;
     WS src;
     if (kStage == 1) {
-      if (lane == 0 && gi + nw < a.n_groups) {
-        const DecodeGroup dn = a.groups[gi + nw];
+      if (lane == 0 && gnext < a.n_groups) {
+        const DecodeGroup dn = a.groups[gnext];
         const uint64_t hi = min(dn.w0 + dn.wn, a.wend);
         if (hi > dn.w0) prefetch_l2(g.words + dn.w0, (hi - dn.w0) * 4);
       }
@@ -1213,12 +1237,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
       // receives the next group's span while this one is decoded
       fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0 && gi + nw < a.n_groups) issue(gi + nw, b ^ 1u);
+      if (lane == 0 && gnext < a.n_groups) issue(gnext, b ^ 1u);
       if (!__all_sync(kFull, mbar_wait(wbar + b, phase[b], kBulkWaitTries))) {
         if (lane == 0) set_error(a.err, kErrTimeout);
         // neither copy may still write the buffers when the warp leaves
         mbar_wait(wbar + b, phase[b], kBulkWaitTries);
-        if (gi + nw < a.n_groups) mbar_wait(wbar + (b ^ 1u), phase[b ^ 1u], kBulkWaitTries);
+        if (gnext < a.n_groups) mbar_wait(wbar + (b ^ 1u), phase[b ^ 1u], kBulkWaitTries);
         break;
       }
       phase[b] ^= 1u;
@@ -1376,9 +1400,17 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
       __syncwarp();
     }
     if (ritems && r.pos() > end) bad = true;
-    // interval segments: one (left, len) pair per lane per round; the warp
-    // expands the round's intervals together (an interval can hold thousands
-    // of ids), each lane taking every 32nd id of the concatenation
+    // interval segments: one (left, len) pair per lane per round, expanded by
+    // the whole warp (an interval can hold thousands of ids).  A round with
+    // few intervals copies them one after another, 32 consecutive ids per
+    // step (a broadcast of the interval, then coalesced label loads and
+    // stores); a round with many short ones expands their concatenation,
+    // each lane taking every 32nd id and finding its interval by a search
+    // over the lanes' scan.  The round takes the form with the lower
+    // estimated instruction count: per interval 16 + 4 per 32 ids, against
+    // 100 per 128 ids of the concatenation.  At R-MAT scale 24 (BFS order,
+    // 2.5 % of compressed arcs in intervals) the one-at-a-time form took the
+    // pre-pass from 3.14 to 2.93 ms.
     if (__any_sync(kFull, coop)) {
       uint32_t left_todo = 0, nextbase = 0, w = 0;
       if (coop) {
@@ -1403,30 +1435,53 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
         const uint32_t incl2 = warp_incl_scan(len, lane);
         const uint32_t tot = __shfl_sync(kFull, incl2, 31);
         const uint64_t dst = obase + w;  // where this lane's interval goes
-        // 4 ids per lane per step, their loads in flight together
-        for (uint32_t i0 = 0; i0 < tot; i0 += 128) {
-          uint32_t lv[4];
-          uint64_t at[4];
+        const uint32_t solo = __reduce_add_sync(kFull, len ? 16u + 4u * ((len + 31u) >> 5) : 0u);
+        if (solo <= 100u * ((tot + 127u) >> 7)) {
+          for (uint32_t m = __ballot_sync(kFull, len != 0u); m; m &= m - 1u) {
+            const uint32_t l = uint32_t(__ffs(m) - 1);
+            const uint32_t lo_l = __shfl_sync(kFull, lo, l), len_l = __shfl_sync(kFull, len, l);
+            const uint64_t d_l = (uint64_t(__shfl_sync(kFull, uint32_t(dst >> 32), l)) << 32) |
+                                 __shfl_sync(kFull, uint32_t(dst), l);
+            for (uint32_t k0 = 0; k0 < len_l; k0 += 128) {
+              uint32_t lv[4];
 #pragma unroll
-          for (int u = 0; u < 4; u++) {
-            const uint32_t i = i0 + 32u * u + lane;
-            uint32_t ow = 0;
+              for (int u = 0; u < 4; u++) {
+                const uint32_t k = k0 + 32u * u + lane;
+                lv[u] = k < len_l ? ld_label(c, lo_l + k) : 0u;
+              }
 #pragma unroll
-            for (uint32_t st = 16; st; st >>= 1) {
-              const uint32_t v = __shfl_sync(kFull, incl2, ow + st - 1);
-              if (v <= i) ow += st;
+              for (int u = 0; u < 4; u++) {
+                const uint32_t k = k0 + 32u * u + lane;
+                if (k < len_l) a.scratch[d_l + k] = lv[u];
+              }
             }
-            ow &= 31u;
-            const uint32_t first = __shfl_sync(kFull, incl2 - len, ow);
-            const uint32_t olo = __shfl_sync(kFull, lo, ow);
-            const uint64_t odst = (uint64_t(__shfl_sync(kFull, uint32_t(dst >> 32), ow)) << 32) |
-                                  __shfl_sync(kFull, uint32_t(dst), ow);
-            at[u] = odst + (i - first);
-            lv[u] = i < tot ? ld_label(c, olo + (i - first)) : 0u;
           }
+        } else {
+          // 4 ids per lane per step, their loads in flight together
+          for (uint32_t i0 = 0; i0 < tot; i0 += 128) {
+            uint32_t lv[4];
+            uint64_t at[4];
 #pragma unroll
-          for (int u = 0; u < 4; u++)
-            if (i0 + 32u * u + lane < tot) a.scratch[at[u]] = lv[u];
+            for (int u = 0; u < 4; u++) {
+              const uint32_t i = i0 + 32u * u + lane;
+              uint32_t ow = 0;
+#pragma unroll
+              for (uint32_t st = 16; st; st >>= 1) {
+                const uint32_t v = __shfl_sync(kFull, incl2, ow + st - 1);
+                if (v <= i) ow += st;
+              }
+              ow &= 31u;
+              const uint32_t first = __shfl_sync(kFull, incl2 - len, ow);
+              const uint32_t olo = __shfl_sync(kFull, lo, ow);
+              const uint64_t odst = (uint64_t(__shfl_sync(kFull, uint32_t(dst >> 32), ow)) << 32) |
+                                    __shfl_sync(kFull, uint32_t(dst), ow);
+              at[u] = odst + (i - first);
+              lv[u] = i < tot ? ld_label(c, olo + (i - first)) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+              if (i0 + 32u * u + lane < tot) a.scratch[at[u]] = lv[u];
+          }
         }
         w += len;
       }
@@ -1606,7 +1661,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
   if (lane == 0) mbar_init(s_bar + warp, 1u);
   fence_mbar_init();
   __syncthreads();
-  uint32_t *qctr = a.work + 4 * (a.it_dev ? c.it : 0u) + 2;
+  uint32_t *qctr = a.work + kWorkCounters * (a.it_dev ? c.it : 0u) + kWqBlock;
   unsigned long long changed = 0;
 
   // Block items, claimed ahead: while the block works on item k, thread 0

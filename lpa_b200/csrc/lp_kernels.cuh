@@ -52,6 +52,8 @@ struct DecodeGroup {
   uint32_t wn, pad;
 };
 constexpr uint32_t kDecodeWindow = 768;  // staged ids per warp of the pre-pass
+// decode groups a warp of the pre-pass claims from its work queue at once
+constexpr uint32_t kGroupClaim = 4;
 // lpa_tune.stage_stream 2: words of a group's stream span one shared-memory
 // buffer holds (32 segments of < 512 bits plus their headers fit)
 constexpr uint32_t kSpanWords = 576;
@@ -95,13 +97,18 @@ constexpr uint32_t kPackedMaxDeg = 15;  // the tiny bucket (degree < 16)
 
 constexpr int kBusyKernels = 4;  // kernels of an iteration with a busy span (IterArgs::ktime)
 
+// Work-queue counters of one iteration (IterArgs::work + kWorkCounters *
+// slot): k_iterate's heavy items and light chunks, the count pass's block and
+// warp items, the pre-pass's decode groups; the rest unused.
+enum WorkCounter : int { kWqHeavy = 0, kWqLight, kWqBlock, kWqWarp, kWqGroups, kWorkCounters = 8 };
+
 struct IterArgs {
   DevGraph g;
   uint32_t *labs0, *labs1;      // the two label buffers
   uint32_t parity0;             // iteration 0 of this launch reads labs0 when 0, labs1 when 1
   const uint32_t *it_dev;       // device iteration counter (CUDA-graph loop), nullptr: 0
   unsigned long long *changed;  // changed counters, indexed by the iteration counter
-  uint32_t *work;               // work-queue counters, indexed by the iteration counter
+  uint32_t *work;               // work-queue counters: kWorkCounters per iteration slot
   uint32_t *err;
   const Seg *segs;              // all segments
   const uint8_t *seg_var;       // variant per segment

@@ -300,9 +300,10 @@ static void upload_lists(lpa_handle *h) {
   h->n_cwarp = out.n_cwarp;
   ensure_hub_spill(h);
   h->plan_version++;
-  // one warp per decode group, kThreads / 32 warps per block
+  // the resident blocks (the warps take decode groups from a work queue),
+  // fewer when there are fewer groups than warps
   h->grid_decode = int(std::max<uint64_t>(
-      1, std::min<uint64_t>((uint64_t(h->n_groups) + kWarps - 1) / kWarps, uint64_t(h->num_sms) * 8)));
+      1, std::min<uint64_t>((uint64_t(h->n_groups) + kWarps - 1) / kWarps, uint64_t(h->num_sms) * h->occ_decode)));
 }
 
 // The work lists of every range of a streamed handle, each built by the
@@ -371,7 +372,7 @@ static void upload_range_lists(lpa_handle *h) {
     r.n_cblock = out.n_cblock;
     r.n_cwarp = out.n_cwarp;
     r.grid_decode = int(std::max<uint64_t>(
-        1, std::min<uint64_t>((uint64_t(r.n_groups) + kWarps - 1) / kWarps, uint64_t(h->num_sms) * 8)));
+        1, std::min<uint64_t>((uint64_t(r.n_groups) + kWarps - 1) / kWarps, uint64_t(h->num_sms) * h->occ_decode)));
     h->n_heavy += r.n_heavy;
     h->n_light += r.n_light;
     h->n_packed += r.n_packed;
@@ -465,6 +466,9 @@ static void build_ranges(lpa_handle *h) {
   cur.s1 = S;  // the small CSR's segments too
   cur.last = true;
   h->ranges.push_back(cur);
+  // every range takes one block of work-queue counters per iteration
+  if (h->ranges.size() > size_t(kMaxRunSlots))
+    throw Fail{LPA_ERR_CAPACITY, "stream budget too small: more ranges than work-counter slots"};
   for (StreamRange &r : h->ranges) {
     words_of(h, off, r.p0, std::max(r.p1, r.p0), r.w0, r.w1);
     r.a0 = arc[r.p0];
@@ -715,7 +719,7 @@ static void enqueue_streamed_iteration(lpa_handle *h, unsigned long long *change
     const StreamRange &r = h->ranges[k];
     const int b = int(k & 1);
     check(h, cudaStreamWaitEvent(h->stream, h->ev_ready[b], 0), "wait for the stream range");
-    IterArgs a = iter_args(h, changed, work + 4 * k);
+    IterArgs a = iter_args(h, changed, work + kWorkCounters * k);
     a.g.words = base[k];
     a.heavy = r.items;
     a.n_heavy = r.n_heavy;
@@ -871,6 +875,7 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     h->grid_count = h->num_sms * std::max(1, occ_count);
     int occ_decode = 1;  // one grid for every form
     check(h, occupancy_decode_two_pass(&occ_decode), "occupancy");
+    h->occ_decode = std::max(1, occ_decode);
     // 960 is divisible by every resident warp count these kernels reach (16..64 in steps of 8)
     const auto weight = [](int blocks) { return uint32_t(std::max(1, 960 / (std::max(1, blocks) * kWarps))); };
     h->cw_iterate = weight(h->occ);
@@ -923,8 +928,8 @@ lpa_status lpa_create(const lpa_graph_desc *g, const lpa_opts *o, lpa_handle **o
     h->d_lab[1] = dalloc<uint32_t>(h, n, "labels");
     h->changed_slots = kMaxRunSlots;
     h->d_changed = dalloc<unsigned long long>(h, h->changed_slots, "changed counters");
-    h->d_work = dalloc<uint32_t>(h, 4 * size_t(h->changed_slots), "work counters");
-    check(h, cudaMemsetAsync(h->d_work, 0, 4 * size_t(h->changed_slots) * sizeof(uint32_t), h->stream),
+    h->d_work = dalloc<uint32_t>(h, kWorkCounters * size_t(h->changed_slots), "work counters");
+    check(h, cudaMemsetAsync(h->d_work, 0, kWorkCounters * size_t(h->changed_slots) * sizeof(uint32_t), h->stream),
           "clear work counters");
     check(h, cudaMemsetAsync(h->d_changed, 0, h->changed_slots * sizeof(unsigned long long), h->stream),
           "clear counters");
@@ -1041,7 +1046,7 @@ lpa_status lpa_iterate(lpa_handle *h, uint64_t *changed_out) {
     unsigned long long *slot = h->d_changed;
     check(h, cudaMemsetAsync(slot, 0, sizeof(unsigned long long), h->stream), "clear counter");
     const size_t slots = h->streamed ? std::max<size_t>(1, h->ranges.size()) : 1;  // a counter block per range
-    check(h, cudaMemsetAsync(h->d_work, 0, 4 * slots * sizeof(uint32_t), h->stream), "clear work counters");
+    check(h, cudaMemsetAsync(h->d_work, 0, kWorkCounters * slots * sizeof(uint32_t), h->stream), "clear work counters");
     enqueue_iteration(h, slot, h->d_work);
     check(h, cudaGetLastError(), "iteration launch");
     check(h, cudaMemcpyAsync(h->h_pinned, slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream),
@@ -1239,7 +1244,7 @@ static double tune_trial(lpa_handle *h, int repeats) {
           "clear spans");
     check(h, cudaMemsetAsync(h->d_changed, 0, sizeof(unsigned long long), h->stream), "clear counter");
     const size_t slots = h->streamed ? std::max<size_t>(1, h->ranges.size()) : 1;
-    check(h, cudaMemsetAsync(h->d_work, 0, 4 * slots * sizeof(uint32_t), h->stream), "clear work counters");
+    check(h, cudaMemsetAsync(h->d_work, 0, kWorkCounters * slots * sizeof(uint32_t), h->stream), "clear work counters");
     enqueue_iteration(h, h->d_changed, h->d_work);
     h->cur = cur;
     check(h, cudaGetLastError(), "tuning iteration");

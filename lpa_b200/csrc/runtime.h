@@ -121,7 +121,8 @@ struct lpa_handle {
   int grid = 0;          // persistent iteration kernel
   int grid_decode = 0;   // two-pass decode kernel
   int occ = 1;
-  uint32_t *d_work = nullptr;        // two queue counters per iteration slot
+  int occ_decode = 1;    // resident blocks per SM of the two-pass decode kernel
+  uint32_t *d_work = nullptr;        // kWorkCounters queue counters per iteration slot
   uint32_t *d_seg_changed = nullptr; // per-segment changed counts (cost-model feature)
   uint32_t *d_seg_changed_prev = nullptr;  // the previous iteration's
 
