@@ -1203,10 +1203,14 @@ __global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
 // copy of group k + 1 overlaps the decode of group k; the lanes then read
 // their words from the buffer (words outside the copied span, if any, from
 // the stream itself).
-template <int kGather, int kStage>
+//
+// kPack (n <= 2^27, unstaged forms): a staged id carries its lane in its top
+// 5 bits, so the window needs no owner bytes (one shared store per id fewer:
+// pre-pass 2.45 -> 2.39 ms at R-MAT scale 24).
+template <int kGather, int kStage, bool kPack>
 __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   __shared__ uint32_t stage[kWarps * kDecodeWindow];
-  __shared__ uint8_t owner[kWarps * kDecodeWindow];
+  __shared__ uint8_t owner[kPack ? 1 : kWarps * kDecodeWindow];
   extern __shared__ __align__(16) uint32_t sspan[];  // kStage 2: kSpanSmemBytes of dynamic shared memory
   __shared__ uint64_t sbar[kStage == 2 ? kWarps * 2 : 1];
   using WS = typename std::conditional<kStage == 2, StagedWords, GWords>::type;
@@ -1385,8 +1389,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
                         __shfl_sync(kFull, uint32_t(obase), 0);
     const bool rel32 = __all_sync(kFull, ritems == 0u || ((obase + ritems - gb) >> 32) == 0ull);
     const uint32_t drel = uint32_t(obase - gb) - rexcl;
+    const uint32_t nmax = uint32_t(g.n - 1);
     uint32_t *wst = stage + warp * kDecodeWindow;
-    uint8_t *wown = owner + warp * kDecodeWindow;
+    uint8_t *wown = owner + (kPack ? 0u : warp * kDecodeWindow);
     uint32_t done = 0, v = 0;
     for (uint32_t w0 = 0; w0 < rtot; w0 += kDecodeWindow) {
       const uint32_t w1 = min(w0 + kDecodeWindow, rtot);
@@ -1394,32 +1399,37 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
       // index rexcl + i - w0 (>= 0 for every item not yet written)
       const uint32_t lim = rexcl + done < w1 ? min(ritems, w1 - rexcl) : done;
       uint32_t *dst = wst + (int32_t(rexcl) - int32_t(w0));
-      uint8_t *own = wown + (int32_t(rexcl) - int32_t(w0));
-      bool oob = false;
+      // staged: the id (clamped to n - 1, so every gather stays in bounds),
+      // with its lane in the top bits (kPack) or in the owner bytes
+      const auto put = [&](uint32_t k, uint32_t id) {
+        if constexpr (kPack) {
+          dst[k] = min(id, nmax) | (lane << 27);
+        } else {
+          dst[k] = min(id, nmax);
+          wown[int32_t(rexcl) - int32_t(w0) + int32_t(k)] = uint8_t(lane);
+        }
+      };
       if (done == 0 && lim > 0) {
         v = zigzag_first(node, r.zeta3(bad));
-        oob |= uint64_t(v) >= g.n;
-        dst[0] = oob ? node : v;
-        own[0] = uint8_t(lane);
+        put(0, v);
         done = 1;
       }
       for (; done < lim; done++) {
         v += r.zeta3(bad) + 1u;
-        // an id out of range reads the vertex's own label; the error word
-        // reports the stream (its end is checked once, below)
-        const bool out = uint64_t(v) >= g.n;
-        oob |= out;
-        dst[done] = out ? node : v;
-        own[done] = uint8_t(lane);
+        put(done, v);
       }
-      bad |= oob;
+      // a segment's ids ascend, so its last one is its largest: an id past
+      // n - 1 read label n - 1, and the error word reports the stream (its end
+      // is checked once, below).  Clamping instead of testing every id took
+      // the pre-pass from 2.49 to 2.45 ms at R-MAT scale 24.
+      if (done) bad |= v > nmax;
       __syncwarp();
       for (uint32_t f0 = w0; f0 < w1; f0 += 256) {
         uint32_t lv[8];
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           const uint32_t f = f0 + 32u * u + lane;
-          const uint32_t id = f < w1 ? wst[f - w0] : 0u;
+          const uint32_t id = f < w1 ? (kPack ? wst[f - w0] & 0x07FFFFFFu : wst[f - w0]) : 0u;
           lv[u] = f >= w1 ? 0u
                   : (kGather == 2 || (kGather == 0 && id < hot)) ? __ldg(c.lab_in + id)
                                                                   : __ldcg(c.lab_in + id);
@@ -1428,7 +1438,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
 #pragma unroll
           for (int u = 0; u < 8; u++) {
             const uint32_t f = f0 + 32u * u + lane;
-            const uint32_t ol = f < w1 ? wown[f - w0] : 0u;
+            const uint32_t ol = f < w1 ? (kPack ? wst[f - w0] >> 27 : wown[f - w0]) : 0u;
             const uint32_t rel = __shfl_sync(kFull, drel, ol) + f;
             if (f < w1) a.scratch[gb + rel] = lv[u];
           }
@@ -1436,7 +1446,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
 #pragma unroll
           for (int u = 0; u < 8; u++) {
             const uint32_t f = f0 + 32u * u + lane;
-            const uint32_t ol = f < w1 ? wown[f - w0] : 0u;
+            const uint32_t ol = f < w1 ? (kPack ? wst[f - w0] >> 27 : wown[f - w0]) : 0u;
             const uint64_t ob = (uint64_t(__shfl_sync(kFull, uint32_t(obase >> 32), ol)) << 32) |
                                 __shfl_sync(kFull, uint32_t(obase), ol);
             const uint32_t ox = __shfl_sync(kFull, rexcl, ol);
@@ -1542,10 +1552,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   busy_mark(a, 0, true);
 }
 
-#define LPA_DECODE_FORMS(G)                                  \
-  template __global__ void k_decode_two_pass<G, 0>(IterArgs a); \
-  template __global__ void k_decode_two_pass<G, 1>(IterArgs a); \
-  template __global__ void k_decode_two_pass<G, 2>(IterArgs a);
+#define LPA_DECODE_FORMS(G)                                           \
+  template __global__ void k_decode_two_pass<G, 0, false>(IterArgs a); \
+  template __global__ void k_decode_two_pass<G, 1, false>(IterArgs a); \
+  template __global__ void k_decode_two_pass<G, 2, false>(IterArgs a); \
+  template __global__ void k_decode_two_pass<G, 0, true>(IterArgs a);
 LPA_DECODE_FORMS(0)
 LPA_DECODE_FORMS(1)
 LPA_DECODE_FORMS(2)
@@ -1923,18 +1934,19 @@ template __global__ void k_count_two_pass<true>(IterArgs a);
 
 template <int G>
 static void launch_decode_form(uint32_t stage, int grid, cudaStream_t s, const IterArgs &a) {
-  if (stage == 1) k_decode_two_pass<G, 1><<<grid, kThreads, 0, s>>>(a);
-  else if (stage == 2) k_decode_two_pass<G, 2><<<grid, kThreads, kSpanSmemBytes, s>>>(a);
-  else k_decode_two_pass<G, 0><<<grid, kThreads, 0, s>>>(a);
+  if (stage == 1) k_decode_two_pass<G, 1, false><<<grid, kThreads, 0, s>>>(a);
+  else if (stage == 2) k_decode_two_pass<G, 2, false><<<grid, kThreads, kSpanSmemBytes, s>>>(a);
+  else if (a.g.n <= (1ull << 27)) k_decode_two_pass<G, 0, true><<<grid, kThreads, 0, s>>>(a);
+  else k_decode_two_pass<G, 0, false><<<grid, kThreads, 0, s>>>(a);
 }
 
 cudaError_t prepare_decode_two_pass() {
-  cudaError_t e = cudaFuncSetAttribute(k_decode_two_pass<0, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_decode_two_pass<0, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(kSpanSmemBytes));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_decode_two_pass<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSpanSmemBytes));
+    e = cudaFuncSetAttribute(k_decode_two_pass<1, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSpanSmemBytes));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_decode_two_pass<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSpanSmemBytes));
+    e = cudaFuncSetAttribute(k_decode_two_pass<2, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSpanSmemBytes));
   return e;
 }
 
@@ -1953,9 +1965,9 @@ cudaError_t occupancy_decode_two_pass(int *blocks) {
   // the forms without shared-memory staging (the default); the staged form
   // holds more shared memory and runs fewer blocks per SM
   int b0 = 1, b1 = 1, b2 = 1;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_decode_two_pass<0, 0>, kThreads, 0);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_decode_two_pass<1, 0>, kThreads, 0);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_decode_two_pass<2, 0>, kThreads, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_decode_two_pass<0, 0, false>, kThreads, 0);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_decode_two_pass<1, 0, false>, kThreads, 0);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_decode_two_pass<2, 0, false>, kThreads, 0);
   *blocks = b0 < b1 ? (b0 < b2 ? b0 : b2) : (b1 < b2 ? b1 : b2);
   return e;
 }

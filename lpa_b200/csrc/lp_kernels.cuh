@@ -215,8 +215,10 @@ __global__ void k_batch(BatchArgs b);
 __global__ void k_batch_init(const BatchGraph *graphs, uint32_t ngraphs);
 
 __global__ void k_iterate(IterArgs a);
-// kGather: the cache path of the residual label reads (lpa_tune.gather_cache)
-template <int kGather, int kStage>
+// kGather: the cache path of the residual label reads (lpa_tune.gather_cache);
+// kStage: the stream staging (lpa_tune.stage_stream); kPack: staged ids carry
+// their lane (n <= 2^27, unstaged forms)
+template <int kGather, int kStage, bool kPack>
 __global__ void k_decode_two_pass(IterArgs a);
 // V2 for tiny vertices: a lane per vertex.
 __global__ void k_packed(IterArgs a);
@@ -227,7 +229,7 @@ __global__ void k_count_two_pass(IterArgs a);
 
 // The template forms of the two-pass kernels are launched and sized only in
 // the file that defines them (lp_kernels.cu):
-// k_decode_two_pass<gather_cache, stage_stream> on `grid` blocks of kThreads;
+// k_decode_two_pass<gather_cache, stage_stream, pack> on `grid` blocks of kThreads;
 void launch_decode_two_pass(uint32_t gather_cache, uint32_t stage, int grid, cudaStream_t s, const IterArgs &a);
 // k_count_two_pass<bulk> on `grid` blocks of kThreads with kCountSmemBytes;
 void launch_count_two_pass(bool bulk, int grid, cudaStream_t s, const IterArgs &a);
