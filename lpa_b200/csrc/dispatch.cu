@@ -336,6 +336,7 @@ bool lpa_learner_settled(lpa_handle *h) {
 
 void lpa_learner_before_iteration(lpa_handle *h) {
   h->collect_cycles = false;
+  h->learner_spans = false;
   if (h->opts.dispatch != LPA_DISPATCH_LEARNED) return;
   if (!h->learner && !learner_setup(h)) {
     lpa_learner_free(h);
@@ -362,8 +363,14 @@ void lpa_learner_before_iteration(lpa_handle *h) {
       plan = (L->since_check >= kRecheck) ? L->learned : h->fixed;
   }
   set_plan(h, plan);
-  h->collect_cycles = true;
-  cudaMemsetAsync(h->d_seg_cycles, 0, std::max<size_t>(1, h->segs.size()) * sizeof(long long), h->stream);
+  // per-segment cycles only while the model trains on them (every item's
+  // booking is an atomic); every phase times the iteration by its kernels'
+  // busy spans
+  const bool training = L->phase == kPhaseFixed || L->phase == kPhaseExplore;
+  h->collect_cycles = training;
+  h->learner_spans = true;
+  if (training)
+    cudaMemsetAsync(h->d_seg_cycles, 0, std::max<size_t>(1, h->segs.size()) * sizeof(long long), h->stream);
   cudaMemsetAsync(h->d_ktime, 0xFF, lpa_dev::kBusyKernels * sizeof(unsigned long long), h->stream);  // starts
   cudaMemsetAsync(h->d_ktime + lpa_dev::kBusyKernels, 0, lpa_dev::kBusyKernels * sizeof(unsigned long long),
                   h->stream);  // ends
@@ -373,6 +380,7 @@ void lpa_learner_before_iteration(lpa_handle *h) {
 
 void lpa_learner_after_iteration(lpa_handle *h) {
   h->collect_cycles = false;
+  h->learner_spans = false;
   Learner *L = h->learner;
   if (!L || h->opts.dispatch != LPA_DISPATCH_LEARNED) return;
   // The yardstick's clock: the time the iteration's kernels were busy on the GPU

@@ -620,7 +620,7 @@ static IterArgs iter_args(lpa_handle *h, unsigned long long *changed, uint32_t *
   a.cw_iterate = h->cw_iterate;
   a.cw_decode = h->cw_decode;
   a.cw_count = h->cw_count;
-  a.ktime = (h->collect_cycles || h->measure_busy) ? h->d_ktime : nullptr;
+  a.ktime = (h->collect_cycles || h->measure_busy || h->learner_spans) ? h->d_ktime : nullptr;
   a.seg_changed = h->learner ? h->d_seg_changed : nullptr;
   a.cms_thr = h->opts.cms_threshold;
   for (int r = 0; r < kCmsDepth; r++) a.seeds[r] = h->seeds[r];

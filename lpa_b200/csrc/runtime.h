@@ -70,6 +70,7 @@ struct lpa_handle {
   lpa_opts opts{};
   lpa_tune tune{32, 4, lpa_dev::kCountWarpMax, 2, 0, 0, 0};  // count-pass work shapes (lpa_set_tune / lpa_autotune)
   bool measure_busy = false;                        // record kernel busy spans (IterArgs::ktime)
+  bool learner_spans = false;                       // the same, for the learned dispatch's iteration clock
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
