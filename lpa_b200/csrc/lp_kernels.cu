@@ -411,16 +411,21 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
       const uint32_t batch = __ballot_sync(kFull, in_batch);
       const uint32_t total = __shfl_sync(kFull, incl, 31 - __clz(batch));
       if (in_batch) {
+        // ids are clamped to n - 1, so every gather stays in range; a
+        // segment's ids ascend, so its last one is its largest, and it and the
+        // segment's end are tested once, after the last code (the stream was
+        // validated code by code when the handle was created)
+        const uint32_t nmax = uint32_t(g.n - 1);
         uint32_t o = incl - sc, v = 0;
-        for (uint32_t cc = 0; cc < cnt; cc++) {
-          const uint32_t x = r.zeta3(bad);
-          v = (cc == 0) ? zigzag_first(node, x) : v + x + 1u;
-          if (bad || r.pos() > end || uint64_t(v) >= g.n) {
-            bad = true;
-            v = node;  // keeps the staged id in range; the error word reports the stream
-          }
-          wst[o++] = v;
+        if (cnt) {
+          v = zigzag_first(node, r.zeta3(bad));
+          wst[o++] = min(v, nmax);
         }
+        for (uint32_t cc = 1; cc < cnt; cc++) {
+          v += r.zeta3(bad) + 1u;
+          wst[o++] = min(v, nmax);
+        }
+        if (cnt && (v > nmax || r.pos() > end)) bad = true;
         my_items += cnt;
         if (j == nseg_r - 1) sh.last_end = r.pos();
       }
@@ -667,15 +672,21 @@ __device__ bool warp_decode_batch(const DevGraph &g, uint32_t *stage, bool activ
     const uint32_t at_fo = __shfl_sync(kFull, c_excl, fo);
     if (has && !bad) {
       const uint32_t rel = io + rdo + (c_excl - at_fo);  // item offset inside the owner's region
-      uint32_t v = 0;
-      for (uint32_t c = 0; c < cnt; c++) {
-        const uint32_t x = rr.zeta3(bad);
-        v = (c == 0) ? zigzag_first(ndo, x) : v + x + 1u;
-        if (bad || rr.pos() > en || uint64_t(v) >= g.n || rel + c >= dd) {
-          bad = true;
-          break;
+      if (uint64_t(rel) + cnt > dd) {
+        bad = true;
+      } else {
+        // clamped ids, one range and end test per segment (as heavy_produce)
+        const uint32_t nmax = uint32_t(g.n - 1);
+        uint32_t v = 0;
+        if (cnt) {
+          v = zigzag_first(ndo, rr.zeta3(bad));
+          stage[bo + rel] = min(v, nmax);
         }
-        stage[bo + rel + c] = v;
+        for (uint32_t c = 1; c < cnt; c++) {
+          v += rr.zeta3(bad) + 1u;
+          stage[bo + rel + c] = min(v, nmax);
+        }
+        if (cnt && (v > nmax || rr.pos() > en)) bad = true;
       }
       if (j == no - 1 && rr.pos() != en) bad = true;
     }
