@@ -1916,6 +1916,9 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
           const EpochTable et{wslots, min(next_pow2(2 * d), kCountWarpSlots), wepoch};
           uint64_t bp = 0;
           if (ids) count_exact(et, g.small_nbr + g.small_off[p - g.n_c], d, 0, 1, bp, c.lab_in);
+          // a vertex of at most 128 labels loads them in one step of four rows
+          // rather than eight (count pass 2.26 -> 2.21 ms at R-MAT scale 24)
+          else if (d <= 128) count_exact<4>(et, a.scratch + a.arc_off[p], d, 0, 1, bp);
           else count_exact(et, a.scratch + a.arc_off[p], d, 0, 1, bp);
           bp = warp_max_u64(bp);
           if (lane == 0) {
