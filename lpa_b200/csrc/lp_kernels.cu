@@ -1126,7 +1126,7 @@ __device__ __forceinline__ uint32_t packed_vertex(const IterArgs &a, const Ctx &
     // the walk stages the ids, then every label load is in flight at once (a
     // load in the walk's loop held the lane at its store: road grid 1404^2,
     // k_packed 0.096 -> 0.079 ms)
-    const int64_t r = walk_vertex_buf(g.words, g.offsets[p], g.offsets[p + 1], node, g.n, [&](uint32_t id) {
+    const int64_t r = walk_vertex_buf<true>(g.words, g.offsets[p], g.offsets[p + 1], node, g.n, [&](uint32_t id) {
       if (k < kPackedMaxDeg) lab[k] = id;
       k++;
     });
