@@ -364,21 +364,27 @@ void lpa_learner_before_iteration(lpa_handle *h) {
   }
   set_plan(h, plan);
   // per-segment cycles only while the model trains on them (every item's
-  // booking is an atomic); every phase times the iteration by its kernels'
-  // busy spans
+  // booking is an atomic); the iteration is timed by its kernels' busy spans
+  // until the plan is chosen, then only on the iteration before a recheck
+  // and on the recheck itself (the spans' atomics cost a 15 us iteration of
+  // the road grid 362^2 about a quarter)
   const bool training = L->phase == kPhaseFixed || L->phase == kPhaseExplore;
+  const bool settled = L->phase == kPhaseLearned || L->phase == kPhaseReverted;
   h->collect_cycles = training;
-  h->learner_spans = true;
+  h->learner_spans = !settled || L->since_check + 1 >= kRecheck;
   if (training)
     cudaMemsetAsync(h->d_seg_cycles, 0, std::max<size_t>(1, h->segs.size()) * sizeof(long long), h->stream);
-  cudaMemsetAsync(h->d_ktime, 0xFF, lpa_dev::kBusyKernels * sizeof(unsigned long long), h->stream);  // starts
-  cudaMemsetAsync(h->d_ktime + lpa_dev::kBusyKernels, 0, lpa_dev::kBusyKernels * sizeof(unsigned long long),
-                  h->stream);  // ends
+  if (h->learner_spans) {
+    cudaMemsetAsync(h->d_ktime, 0xFF, lpa_dev::kBusyKernels * sizeof(unsigned long long), h->stream);  // starts
+    cudaMemsetAsync(h->d_ktime + lpa_dev::kBusyKernels, 0, lpa_dev::kBusyKernels * sizeof(unsigned long long),
+                    h->stream);  // ends
+  }
   std::swap(h->d_seg_changed, h->d_seg_changed_prev);
   cudaMemsetAsync(h->d_seg_changed, 0, std::max<size_t>(1, h->segs.size()) * sizeof(uint32_t), h->stream);
 }
 
 void lpa_learner_after_iteration(lpa_handle *h) {
+  const bool timed = h->learner_spans;
   h->collect_cycles = false;
   h->learner_spans = false;
   Learner *L = h->learner;
@@ -389,7 +395,9 @@ void lpa_learner_after_iteration(lpa_handle *h) {
   // such as a profiler can stretch by orders of magnitude.
   double t = h->last_iter_ms;
   unsigned long long span[2 * lpa_dev::kBusyKernels];
-  if (cudaMemcpy(span, h->d_ktime, sizeof(span), cudaMemcpyDeviceToHost) == cudaSuccess) {
+  if (!timed) {
+    // a settled plan between rechecks: nothing to compare
+  } else if (cudaMemcpy(span, h->d_ktime, sizeof(span), cudaMemcpyDeviceToHost) == cudaSuccess) {
     double busy = 0;
     for (int k = 0; k < lpa_dev::kBusyKernels; k++)
       if (span[lpa_dev::kBusyKernels + k] > span[k]) busy += double(span[lpa_dev::kBusyKernels + k] - span[k]) * 1e-6;
@@ -452,8 +460,10 @@ void lpa_learner_after_iteration(lpa_handle *h) {
         L->phase = learned_wins ? kPhaseLearned : kPhaseReverted;
         L->since_check = 0;
       } else {
-        if (fixed_now) L->t_fixed = t;
-        else L->t_learned = t;
+        if (timed) {
+          if (fixed_now) L->t_fixed = t;
+          else L->t_learned = t;
+        }
         L->since_check++;
       }
       break;
