@@ -7,6 +7,7 @@
 // callers; a violation sets the device error word (never traps).
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace lpa_dev {
@@ -237,14 +238,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
 // memory).
 template <class WS>
 struct BitReaderT {
+  // a global-memory source is read through a pointer to the next word (a
+  // refill is one load and one pointer step, no index arithmetic)
+  static constexpr bool kPtr = std::is_same<WS, GWords>::value;
   WS w;
-  uint32_t hi, lo;  // upcoming bits, MSB-aligned: hi the next 32, lo the 32 after (zero past the valid bits)
-  uint64_t wnext;   // next word to load
-  uint32_t nb;      // valid bits in hi:lo
+  uint32_t hi, lo;       // upcoming bits, MSB-aligned: hi the next 32, lo the 32 after (zero past the valid bits)
+  uint64_t wnext;        // next word to load (sources other than GWords)
+  const uint32_t *wp;    // GWords: the next word to load
+  uint32_t nb;           // valid bits in hi:lo
 
+  __device__ __forceinline__ uint64_t next_word() const {
+    if constexpr (kPtr) return uint64_t(wp - w.p);
+    else return wnext;
+  }
   // absolute position of the next unread bit (kept implicit: every code
   // would otherwise pay a 64-bit add)
-  __device__ __forceinline__ uint64_t pos() const { return (wnext << 5) - nb; }
+  __device__ __forceinline__ uint64_t pos() const { return (next_word() << 5) - nb; }
   __device__ __forceinline__ void seek(WS words, uint64_t p) {
     w = words;
     const uint64_t i = p >> 5;
@@ -253,15 +262,17 @@ struct BitReaderT {
     hi = __funnelshift_l(b, a, s);
     lo = b << s;
     nb = 64 - s;
-    wnext = i + 2;
+    if constexpr (kPtr) wp = w.p + i + 2;
+    else wnext = i + 2;
   }
   // Tops the buffer up to at least 33 valid bits (from at least 1).
   __device__ __forceinline__ void fill() {
     if (nb <= 32) {  // every valid bit is in hi and lo is zero
-      const uint32_t x = w(wnext);
+      uint32_t x;
+      if constexpr (kPtr) x = __ldg(wp++);
+      else x = w(wnext++);
       hi |= __funnelshift_rc(x, 0u, nb);  // x >> nb, 0 when nb == 32
       lo = x << (32 - nb);
-      wnext++;
       nb += 32;
     }
   }

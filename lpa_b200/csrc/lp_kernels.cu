@@ -1410,13 +1410,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
       // index rexcl + i - w0 (>= 0 for every item not yet written)
       const uint32_t lim = rexcl + done < w1 ? min(ritems, w1 - rexcl) : done;
       uint32_t *dst = wst + (int32_t(rexcl) - int32_t(w0));
-      // staged: the id (clamped to n - 1, so every gather stays in bounds),
-      // with its lane in the top bits (kPack) or in the owner bytes
+      // staged: the id with its lane in the top bits (kPack: the id's low 27
+      // bits, so the lane stays intact) or in the owner bytes; the gather
+      // clamps it to n - 1, once per 32 ids rather than once per code
       const auto put = [&](uint32_t k, uint32_t id) {
         if constexpr (kPack) {
-          dst[k] = min(id, nmax) | (lane << 27);
+          dst[k] = (id & 0x07FFFFFFu) | (lane << 27);
         } else {
-          dst[k] = min(id, nmax);
+          dst[k] = id;
           wown[int32_t(rexcl) - int32_t(w0) + int32_t(k)] = uint8_t(lane);
         }
       };
@@ -1430,9 +1431,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
         put(done, v);
       }
       // a segment's ids ascend, so its last one is its largest: an id past
-      // n - 1 read label n - 1, and the error word reports the stream (its end
-      // is checked once, below).  Clamping instead of testing every id took
-      // the pre-pass from 2.49 to 2.45 ms at R-MAT scale 24.
+      // n - 1 reads label n - 1, and the error word reports the stream (its
+      // end is checked once, below).  Clamping instead of testing every id
+      // took the pre-pass from 2.49 to 2.45 ms at R-MAT scale 24.
       if (done) bad |= v > nmax;
       __syncwarp();
       for (uint32_t f0 = w0; f0 < w1; f0 += 256) {
@@ -1440,7 +1441,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           const uint32_t f = f0 + 32u * u + lane;
-          const uint32_t id = f < w1 ? (kPack ? wst[f - w0] & 0x07FFFFFFu : wst[f - w0]) : 0u;
+          const uint32_t id = f < w1 ? min(kPack ? wst[f - w0] & 0x07FFFFFFu : wst[f - w0], nmax) : 0u;
           lv[u] = f >= w1 ? 0u
                   : (kGather == 2 || (kGather == 0 && id < hot)) ? __ldg(c.lab_in + id)
                                                                   : __ldcg(c.lab_in + id);
