@@ -202,7 +202,7 @@ typedef struct lpa_tune {
   uint32_t bulk_stage;       /* 1: several-vertices warp items stage their labels with one bulk copy
                                 (cp.async.bulk into shared memory) instead of per-lane loads; default 0 */
   uint32_t gather_cache;     /* cache path of the two-pass pre-pass's label reads: 0 (default) the labels
-                                of the lowest n/64 ids through L1, the rest through L2 only; 1 all through
+                                of the lowest 8192 ids through L1, the rest through L2 only; 1 all through
                                 L2 only, leaving L1 to the bitstream; 2 all through L1 (hot labels) */
   uint32_t stage_stream;     /* how the pre-pass moves each decode group's stream span ahead of its decode:
                                 0 (default) not at all (per-lane loads); 1 a bulk prefetch of the next

@@ -1200,9 +1200,12 @@ __global__ void __launch_bounds__(kThreads) k_packed(IterArgs a) {
 // kGather (lpa_tune.gather_cache) picks the cache path of the residual label
 // reads: 1 all through L2 only (ld.global.cg), leaving L1 to the bitstream;
 // 2 all through L1, which pays when a few hot labels take many of the reads;
-// 0 the labels of the lowest n/64 ids through L1 and the rest through L2
-// only, which on R-MAT and the copy model comes within 0.5 % of the better
-// of the two.
+// 0 the labels of the lowest kHotIds ids (BFS order puts the hubs there)
+// through L1 and the rest through L2 only.  A hot set about the size of the
+// L1 left beside the window wins: against the lowest n/64 ids (262,144 at
+// R-MAT scale 24) 8192 took the pre-pass from 2.336 to 2.257 ms at scale 24
+// and the copy-model iteration from 24.75 to 24.34 ms, scale 22 within
+// 0.5 %; 4096 and 16384 measured the same as 8192 at scale 24.
 //
 // kStage (lpa_tune.stage_stream) moves each group's stream span (the words its
 // segments read, DecodeGroup::w0/wn) ahead of its decode with the copy
@@ -1227,7 +1230,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_decode_two_pass(IterArgs a) {
   using WS = typename std::conditional<kStage == 2, StagedWords, GWords>::type;
   const DevGraph &g = a.g;
   const Ctx c = resolve(a);
-  const uint32_t hot = uint32_t(g.n >> 6);  // kGather 0: ids below read through L1
+  const uint32_t hot = uint32_t(min(g.n, uint64_t(kHotIds)));  // kGather 0: ids below read through L1
   busy_mark(a, 0, false);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   // Decode groups come from the iteration's work queue, kGroupClaim at a

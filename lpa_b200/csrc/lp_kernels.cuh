@@ -57,6 +57,9 @@ struct DecodeGroup {
 constexpr uint32_t kDecodeWindow = 1024;
 // decode groups a warp of the pre-pass claims from its work queue at once
 constexpr uint32_t kGroupClaim = 4;
+// lpa_tune.gather_cache 0: the pre-pass reads the labels of ids below this
+// through L1 (32 KB of labels), the others through L2 only
+constexpr uint32_t kHotIds = 8192;
 // lpa_tune.stage_stream 2: words of a group's stream span one shared-memory
 // buffer holds (32 segments of < 512 bits plus their headers fit)
 constexpr uint32_t kSpanWords = 576;
