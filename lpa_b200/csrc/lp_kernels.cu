@@ -50,6 +50,13 @@ __device__ __forceinline__ uint32_t ld_label(const Ctx &c, uint32_t i) {
   return c.coherent ? __ldcg(c.lab_in + i) : __ldg(c.lab_in + i);
 }
 
+// A neighbour's label in a random gather: the lowest kHotIds ids (the hubs,
+// in BFS order) through L1, every other id through L2 only, so that the
+// scattered reads do not push the hot labels out of L1.
+__device__ __forceinline__ uint32_t ld_label_gather(const Ctx &c, uint32_t i) {
+  return (!c.coherent && i < kHotIds) ? __ldg(c.lab_in + i) : __ldcg(c.lab_in + i);
+}
+
 __device__ __forceinline__ Ctx resolve(const IterArgs &a) {
   Ctx c;
   c.it = iter_index(a);
@@ -222,7 +229,7 @@ __device__ __forceinline__ void block_gather_from(uint32_t *stage, const uint32_
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const uint32_t k = k0 + u * kThreads;
-      v[u] = k >= total ? 0u : (src_labels ? __ldcs(src + k) : ld_label(c, __ldg(src + k)));
+      v[u] = k >= total ? 0u : (src_labels ? __ldcs(src + k) : ld_label_gather(c, __ldg(src + k)));
     }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
@@ -435,7 +442,7 @@ __device__ bool heavy_produce(const IterArgs &a, const Ctx &c, BlockSh &sh, uint
 #pragma unroll
         for (int u = 0; u < 8; u++) {
           const uint32_t k = k0 + 32 * u;
-          lv[u] = k < total ? ld_label(c, wst[k]) : 0u;
+          lv[u] = k < total ? ld_label_gather(c, wst[k]) : 0u;
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {
@@ -754,9 +761,9 @@ __device__ void light_chunk(const IterArgs &a, const Ctx &c, uint32_t *stage, un
       for (int u = 0; u < 8; u++) {
         const uint32_t k = k0 + 32 * u;
         v[u] = k >= total ? 0u
-                          : (decode ? ld_label(c, stage[k])
+                          : (decode ? ld_label_gather(c, stage[k])
                                     : (cgr && a.scratch_labels ? __ldcs(src + src_skip + k)
-                                                               : ld_label(c, __ldg(src + src_skip + k))));
+                                                               : ld_label_gather(c, __ldg(src + src_skip + k))));
       }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
@@ -1595,7 +1602,8 @@ __device__ __forceinline__ void warp_stream(const uint32_t *__restrict__ src, ui
     }
     if (labels) {  // src holds ids: gather their labels
 #pragma unroll
-      for (int u = 0; u < U; u++) v[u] = (b0 + 32u * u + lane < d) ? __ldg(labels + v[u]) : 0u;
+      for (int u = 0; u < U; u++)
+        v[u] = (b0 + 32u * u + lane < d) ? (v[u] < kHotIds ? __ldg(labels + v[u]) : __ldcg(labels + v[u])) : 0u;
     }
 #pragma unroll
     for (int u = 0; u < U; u++) {
@@ -1849,7 +1857,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_count_two_pass(IterArgs a) {
             }
             if (ids) {
 #pragma unroll
-              for (int u = 0; u < 8; u++) v[u] = (k0 + 32u * u + lane < total) ? ld_label(c, v[u]) : 0u;
+              for (int u = 0; u < 8; u++) v[u] = (k0 + 32u * u + lane < total) ? ld_label_gather(c, v[u]) : 0u;
             }
 #pragma unroll
             for (int u = 0; u < 8; u++)
